@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 OCT chain backend.
+
+Workload (one step = one pass of the chain over one volume buffer):
+2048 samples x 1024 A-scans x 64 B-scans uint16 per GPU (512 MiB of algorithmic
+traffic), cubic k-linearisation, Gaussian window, dispersion compensation,
+fixed-pattern-noise removal with a profile determined beforehand, float32 log
+output. Inputs are seeded synthetic spectra (octproengine_b200.synth) made on
+the device; they and the outputs (256 MiB each) exceed the 126 MB L2, so no
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0). Under torchrun each rank processes its own
+buffer (weak scaling, no collective on the data path); time is the max over
+ranks of the device time between barriers.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N, ASCANS, BSCANS = 2048, 1024, 64
+METRIC = "A-scans/s (2048-pt chain)"
+UNIT = "A-scans/s"
+WORKLOAD = ("2048 samples x 1024 A-scans x 64 B-scans uint16 per GPU, cubic resampling, Gaussian window, "
+            "dispersion compensation, FPN removal, float32 log output")
+
+
+def bench_spec(interp=None):
+    from octproengine_b200.chain import ChainSpec, CUBIC, GAUSS
+    from octproengine_b200 import synth
+    return ChainSpec(signal_length=N, ascans_per_bscan=ASCANS, bscans_per_buffer=BSCANS, resampling=True,
+                     interpolation=CUBIC if interp is None else interp,
+                     resampling_coeffs=synth.linearising_coeffs(N), windowing=True, window_type=GAUSS,
+                     window_center=0.5, window_fill=0.9, dispersion=True,
+                     dispersion_coeffs=synth.compensating_coeffs(12.0, -6.0), fpn_removal=True,
+                     fpn_bscan_count=1, grayscale_min=30.0, grayscale_max=110.0)
+
+
+def algorithmic_bytes_per_ascan(n=N, in_bytes=2):
+    return n * in_bytes + (n // 2) * 4
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic_per_ascan():
+    """DRAM bytes per A-scan of the chain kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "chain_kernel_n2048_cubic_u16.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        m = re.search(r"dram_bytes_per_ascan:\s*([0-9.]+)", f.read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_run(steps: int, warmup: int, threads: int, bscans_per_thread: int = 1):
+    """Times the reference CPU backend (oracle/_ref, FFT = project shim in
+    float32 mode, not FFTW) on `threads` independent backends, one B-scan of
+    the benchmark workload each per step."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import reflib
+    from octproengine_b200 import synth
+    spec = bench_spec()
+    if not reflib.available():
+        reflib.build()
+    reflib.set_fft_precision("f32")
+    r, w, cs = spec.curves()
+    p = reflib.make_params(N, ASCANS, bscans_per_thread, 2, resampling=True, interpolation=spec.interpolation,
+                           resampling_coeffs=spec.resampling_coeffs, windowing=True, window_type=spec.window_type,
+                           window_center=spec.window_center, window_fill=spec.window_fill, dispersion=True,
+                           dispersion_coeffs=spec.dispersion_coeffs, fpn_removal=True,
+                           grayscale_min=spec.grayscale_min, grayscale_max=spec.grayscale_max)
+    raw = synth.as_numpy(synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=bscans_per_thread,
+                                                          seed=1)), "uint16")
+    prof = np.zeros(N, np.float32)
+    backends = []
+    for _ in range(threads):
+        be = reflib.RefBackend(p)
+        be.set_fpn(prof)
+        backends.append(be)
+
+    def one(i):
+        backends[i].process(raw)
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for _ in range(warmup):
+            list(ex.map(one, range(threads)))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            list(ex.map(one, range(threads)))
+        dt = time.perf_counter() - t0
+    for be in backends:
+        be.close()
+    ascans = steps * threads * ASCANS * bscans_per_thread
+    return ascans / dt, dt, ascans
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    rate, dt, ascans = cpu_reference_run(args.steps, args.warmup, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{threads} x 1 B-scan (1024 A-scans) per step"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{ascans} A-scans: {threads} reference CpuBackend instances in parallel, "
+                                   f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    from octproengine_b200 import synth
+    from octproengine_b200.chain import open_context, LANCZOS
+
+    world, rank, local = dist_setup()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    spec = bench_spec().with_(device=local)
+    M = spec.num_ascans
+    x = synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=BSCANS, seed=100 + rank,
+                                         background_ripple=True), device=dev)
+    out = torch.empty((M, N // 2), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    ctx = open_context(spec)
+    # FPN profile determined once from the first B-scan of the buffer
+    ctx.request_fpn_determination()
+    ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    if ctx.synchronize() != 0:
+        raise RuntimeError("chain kernel reported a device status")
+    ms_step = ms_max / args.steps
+    value = world * M / (ms_step / 1e3)
+
+    # kernel-only launch duration (the one chain kernel per step)
+    kernel_ms = ms / args.steps
+    bytes_launch = M * algorithmic_bytes_per_ascan()
+    achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    tpa = profile_traffic_per_ascan()
+
+    # Lanczos variant and FPN determination frame (same buffer)
+    variants = {}
+    spec_l = spec.with_(interpolation=LANCZOS)
+    ctx_l = open_context(spec_l)
+    ctx_l.set_fpn_profile(ctx.fpn_profile())
+    for _ in range(2):
+        ctx_l.process_device(x.data_ptr(), out.data_ptr(), sp)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = max(3, args.steps // 2)
+    e0.record(stream)
+    for _ in range(reps):
+        ctx_l.process_device(x.data_ptr(), out.data_ptr(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    lms = e0.elapsed_time(e1) / reps
+    variants["lanczos8"] = {"value": M / (lms / 1e3), "unit": UNIT, "ms_per_step": lms,
+                            "hbm_frac": bytes_launch / (lms / 1e3) / 1e9 / peak}
+    ctx_l.close()
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.request_fpn_determination()
+        ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    fms = e0.elapsed_time(e1) / reps
+    variants["fpn_determination_frame"] = {"value": M / (fms / 1e3), "unit": UNIT, "ms_per_step": fms}
+
+    # end to end through the public API with host buffers (pinned), H2D + D2H timed
+    xh = torch.empty((M, N), dtype=torch.int16).pin_memory()
+    xh.copy_(x.cpu())
+    oh = torch.empty((M, N // 2), dtype=torch.float32).pin_memory()
+    raw_np = xh.numpy().view(np.uint16)
+    out_np = oh.numpy()
+    for _ in range(2):
+        ctx.process_host(raw_np, out_np)
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.process_host(raw_np, out_np)
+    e2e_dt = time.perf_counter() - t0
+    tt = torch.tensor([e2e_dt], device=dev)
+    if dist is not None:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = world * M * e2e_steps / float(tt.item())
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, dt, ascans = cpu_reference_run(1, 1, threads)
+        cpu_base = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                    "sample": f"{ascans} A-scans ({threads} reference CpuBackend instances x 1 B-scan of the "
+                              f"workload); FFT = project shim (float32 radix-2), not FFTW"}
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch_ascans": world * M, "l2": "inputs and outputs larger than L2",
+                   "parallelism": f"{world} independent buffers (no collective)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (tpa * M) if tpa else None,
+                     "algorithmic_bytes": bytes_launch},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 2,
+                "d2h_bytes_per_step": M * (N // 2) * 4},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "variants": variants,
+    }
+    if cpu_base:
+        line["cpu_baseline"] = cpu_base
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,171 @@
+/*
+ * ope_b200.h -- C ABI of the B200 (sm_100a) backend for the OCTproEngine
+ * per-A-scan processing chain.
+ *
+ * This is the drop-in boundary. The reference dispatches the chain through the
+ * abstract C++ class ope::ProcessingBackend (src/backends/backend_interface.h:12-165),
+ * selected by ope::Backend in Processor::Impl::createBackend
+ * (src/core/processor.cpp:38-50). Every entry point below replaces one method
+ * of that interface (cited per declaration) with a plain-C call: opaque
+ * handle, plain pointers and sizes, integer status codes. No C++ or torch type
+ * crosses this boundary. The C++ class ope::B200Backend (octproengine_b200/host)
+ * wraps these calls and turns a non-zero status into std::runtime_error /
+ * std::invalid_argument, the reference's error convention
+ * (src/backends/cuda/cuda_backend.cu:14-33, src/core/processor.cpp:136-138).
+ *
+ * Numeric conventions follow the reference:
+ *   - input sample types are ope::DataType values (include/types.h:6-19);
+ *   - interpolation and window types are ope::InterpolationMethod /
+ *     ope::WindowType values (include/processorconfiguration.h:16-29);
+ *   - a buffer is bscans x ascans x samples, A-scans contiguous; the output is
+ *     bscans x ascans x (samples/2) float32;
+ *   - the dispersion curve handed to the backend is 2*N interleaved
+ *     (cos, sin) floats, resampling and window curves are N floats.
+ *
+ * Thread safety: one context may be used from one thread at a time, except
+ * ope_b200_submit / ope_b200_wait / ope_b200_ring_* which are safe between a
+ * producer and a consumer thread.
+ */
+#ifndef OPE_B200_H
+#define OPE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define OPE_B200_API __attribute__((visibility("default")))
+#else
+#define OPE_B200_API
+#endif
+
+#define OPE_B200_ABI_VERSION 1
+
+/* Status codes. */
+#define OPE_B200_OK 0
+#define OPE_B200_E_INVALID (-1)     /* bad argument or configuration */
+#define OPE_B200_E_UNSUPPORTED (-2) /* valid for the reference, not supported here */
+#define OPE_B200_E_CUDA (-3)        /* CUDA runtime error */
+#define OPE_B200_E_TIMEOUT (-4)     /* a bounded wait expired */
+#define OPE_B200_E_STATE (-5)       /* call not valid in the current state */
+#define OPE_B200_E_NOMEM (-6)       /* allocation failed */
+#define OPE_B200_E_DEVICE (-7)      /* a kernel reported an error status */
+
+/* Subset of ope::ProcessorConfiguration (include/processorconfiguration.h:31-180)
+ * the chain reads. Enum-valued fields carry the reference enum values. */
+typedef struct ope_b200_config {
+    int32_t signal_length;     /* DataParameters::signalLength (N)            */
+    int32_t ascans_per_bscan;  /* DataParameters::ascansPerBscan (A)          */
+    int32_t bscans_per_buffer; /* DataParameters::bscansPerBuffer (B)         */
+    int32_t input_dtype;       /* DataParameters::inputDataType (ope::DataType) */
+    int32_t bitshift;          /* DataParameters::bitshift (CUDA backend only) */
+    int32_t resampling_enabled;
+    int32_t interpolation; /* ope::InterpolationMethod */
+    int32_t windowing_enabled;
+    int32_t dispersion_enabled;
+    int32_t dc_removal_enabled; /* BackgroundRemovalParameters::enabled          */
+    int32_t dc_window;          /* BackgroundRemovalParameters::rollingAverageWindowSize */
+    int32_t log_scaling;
+    float grayscale_min;
+    float grayscale_max;
+    float addend;
+    float multiplicator;
+    int32_t fpn_removal;     /* PostProcessingParameters::fixedPatternNoiseRemoval */
+    int32_t fpn_bscan_count; /* ::fixedPatternNoiseBscanCount                  */
+    int32_t fpn_continuous;  /* ::continuousFixedPatternNoiseDetermination     */
+    int32_t post_bg_removal; /* PostProcessingParameters::backgroundRemoval    */
+    float bg_weight;
+    float bg_offset;
+    int32_t bscan_flip;
+    int32_t sinusoidal_correction;
+    int32_t float32_as_uint32; /* 1: read FLOAT32 input as uint32 like the reference
+                                  backends do (cpu_kernels.tpp:47-52); 0: as float */
+    int32_t device;            /* CUDA device ordinal                           */
+    int32_t num_input_buffers; /* host input ring depth (>= 2)                  */
+    int32_t reserved[9];
+} ope_b200_config;
+
+typedef struct ope_b200_ctx ope_b200_ctx;
+
+/* Fills `cfg` with the reference defaults (processorconfiguration.h:49-171). */
+OPE_B200_API void ope_b200_config_default(ope_b200_config* cfg);
+
+/* ---- lifecycle: ProcessingBackend::initialize / cleanup (backend_interface.h:17-18) ---- */
+OPE_B200_API int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out);
+OPE_B200_API void ope_b200_destroy(ope_b200_ctx* ctx);
+/* ProcessingBackend::updateConfig (backend_interface.h:27): non-dimension fields only. */
+OPE_B200_API int ope_b200_update_config(ope_b200_ctx* ctx, const ope_b200_config* cfg);
+/* Last error message of this context (never NULL). */
+OPE_B200_API const char* ope_b200_last_error(const ope_b200_ctx* ctx);
+
+/* ---- hot-swap curves: ProcessingBackend::update{Resampling,Dispersion,Window}Curve
+ *      (backend_interface.h:30-32). Copied; the caller keeps ownership.  Updates are
+ *      ordered after all work already enqueued on the context. ---- */
+OPE_B200_API int ope_b200_set_resampling_curve(ope_b200_ctx* ctx, const float* curve, size_t n);
+OPE_B200_API int ope_b200_set_dispersion_curve(ope_b200_ctx* ctx, const float* cos_sin, size_t n_floats);
+OPE_B200_API int ope_b200_set_window_curve(ope_b200_ctx* ctx, const float* curve, size_t n);
+
+/* ---- processing: ProcessingBackend::process (backend_interface.h:24) ---- */
+/* Device-resident: d_in holds A*B raw A-scans (16-byte aligned), d_out
+ * receives A*B*(N/2) floats. Asynchronous on `stream` (a cudaStream_t; NULL is
+ * the CUDA default stream). */
+OPE_B200_API int ope_b200_process_device(ope_b200_ctx* ctx, const void* d_in, float* d_out, void* stream);
+/* Same for an explicit A-scan count (any count >= 1), for callers that batch. */
+OPE_B200_API int ope_b200_process_device_n(ope_b200_ctx* ctx, const void* d_in, float* d_out, int64_t num_ascans,
+                                           void* stream);
+/* Complex output: the chain up to the inverse DFT (after the fixed-pattern
+ * subtraction, before magnitude/log), bins [0, N/2) of each A-scan as
+ * interleaved (re, im) float pairs -- num_ascans * (N/2) * 8 bytes at d_bins
+ * (8-byte aligned). Replaces the complex stage the reference keeps in
+ * allIfftOutputs (cpu_backend.cpp:231-242); used by autofocus and by tests. */
+OPE_B200_API int ope_b200_process_bins_device(ope_b200_ctx* ctx, const void* d_in, void* d_bins, int64_t num_ascans,
+                                              void* stream);
+/* Host to host, synchronous: copies h_in to the device, runs the chain, copies
+ * the result to h_out and waits. */
+OPE_B200_API int ope_b200_process_host(ope_b200_ctx* ctx, const void* h_in, float* h_out);
+
+/* ---- fixed-pattern noise: ProcessingBackend::{request,set,get}FixedPatternNoise*
+ *      (backend_interface.h:45-47). Profiles are interleaved (re, im) pairs. ---- */
+OPE_B200_API int ope_b200_request_fpn_determination(ope_b200_ctx* ctx);
+OPE_B200_API int ope_b200_set_fpn_profile(ope_b200_ctx* ctx, const float* interleaved, size_t complex_pairs);
+OPE_B200_API int ope_b200_get_fpn_profile(ope_b200_ctx* ctx, float* out, size_t cap_pairs, size_t* pairs);
+
+/* ---- post-process background: ProcessingBackend::requestPostProcessBackgroundRecording /
+ *      set/getPostProcessBackgroundProfile (backend_interface.h:40-42) ---- */
+OPE_B200_API int ope_b200_request_bg_recording(ope_b200_ctx* ctx);
+OPE_B200_API int ope_b200_set_bg_profile(ope_b200_ctx* ctx, const float* profile, size_t n);
+OPE_B200_API int ope_b200_get_bg_profile(ope_b200_ctx* ctx, float* out, size_t cap, size_t* n);
+
+/* Waits for all work of the context, then reads and clears the device status
+ * word (0 = no kernel reported an error). */
+OPE_B200_API int ope_b200_synchronize(ope_b200_ctx* ctx, int32_t* device_status);
+
+/* ---- curve generators: ProcessorConfiguration::generate{Resampling,Dispersion,Window}Curve
+ *      (src/core/processorconfiguration.cpp:438-589) and the phase -> (cos, sin)
+ *      hand-off of Processor::Impl::getDispersionCurve (src/core/processor.cpp:77-99).
+ *      Bit-identical to the reference on x86-64. ---- */
+OPE_B200_API int ope_b200_generate_resampling_curve(int32_t n, const float coeffs[4], float* out);
+OPE_B200_API int ope_b200_generate_dispersion_phase(int32_t n, const float coeffs[4], float* out);
+OPE_B200_API int ope_b200_generate_window_curve(int32_t n, int32_t window_type, float center, float fill,
+                                                float* out);
+OPE_B200_API int ope_b200_phase_to_cos_sin(const float* phase, size_t n, float* out_interleaved);
+
+/* Test hook, no reference counterpart: the next launch of this context skips
+ * its first input copy, so its bounded wait runs out after `timeout_us`; the
+ * kernel then records a status that ope_b200_synchronize / process_host
+ * report, and the context stays usable. */
+OPE_B200_API int ope_b200_test_inject_copy_stall(ope_b200_ctx* ctx, uint32_t timeout_us);
+
+/* ABI version and build information. */
+OPE_B200_API int ope_b200_abi_version(void);
+/* 1 if the library can run on device `device` (an sm_100 GPU is present). */
+OPE_B200_API int ope_b200_device_supported(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPE_B200_H */

@@ -1,0 +1,537 @@
+// C ABI of the B200 chain backend: context, curve tables, launches.
+//
+// Replaces the per-frame work of the reference ProcessingBackend
+// implementations (CpuBackend::Impl::processData, cpu_backend.cpp:169-302;
+// CudaBackend::process, cuda_backend.cu:442-773) with one fused kernel launch
+// per buffer. Host tables derived from the curves are double-buffered on the
+// device: a curve update fills the slot no in-flight launch reads (waiting on
+// that slot's last-use event) and then switches to it, so hot-swaps are
+// ordered against frames already enqueued (the reference CUDA backend is not,
+// cuda_backend.cu:784-828).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ope_b200.h"
+#include "chain_launch.h"
+#include "fpn.h"
+#include "tables.h"
+
+using namespace ope_b200;
+
+namespace {
+
+// ope::DataType values (include/types.h:6-19)
+enum : int {
+    DT_UINT8 = 1, DT_UINT16 = 2, DT_UINT32 = 3, DT_UINT64 = 4, DT_INT8 = 5, DT_INT16 = 6,
+    DT_INT32 = 7, DT_INT64 = 8, DT_FLOAT32 = 9, DT_FLOAT64 = 10
+};
+
+int bytes_of(int dt) {
+    switch (dt) {
+        case DT_UINT8: case DT_INT8: return 1;
+        case DT_UINT16: case DT_INT16: return 2;
+        case DT_UINT32: case DT_INT32: case DT_FLOAT32: return 4;
+        case DT_UINT64: case DT_INT64: case DT_FLOAT64: return 8;
+        default: return 0;
+    }
+}
+
+// Kernel input kind for a reference data type. The reference reads bit depth
+// <= 8 as uint8, <= 16 as uint16 and everything wider as uint32
+// (cpu_kernels.tpp:35-53). 64-bit types are not supported.
+int input_kind(int dt, bool float_as_uint) {
+    switch (dt) {
+        case DT_UINT8: case DT_INT8: return IN_U8;
+        case DT_UINT16: case DT_INT16: return IN_U16;
+        case DT_UINT32: case DT_INT32: return IN_U32;
+        case DT_FLOAT32: return float_as_uint ? IN_U32 : IN_F32;
+        default: return -1;
+    }
+}
+
+struct TableSlot {
+    int2* lin = nullptr;
+    int4* cub = nullptr;
+    int* lzb = nullptr;
+    float* lzw = nullptr;
+    float4* wph = nullptr;
+    cudaEvent_t last_use = nullptr;
+};
+
+}  // namespace
+
+struct ope_b200_ctx {
+    ope_b200_config cfg{};
+    int n = 0;
+    long long m = 0;  // A-scans per buffer
+    int in_kind = 0;
+    int interp = INTERP_NONE;
+    size_t in_bytes = 0, out_bytes = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    std::vector<float> resample, window, cos_sin;
+    bool tables_dirty = true;
+    TableSlot slot[2];
+    int active = -1;
+    float2* d_tw = nullptr;
+    int* d_status = nullptr;
+
+    // fixed-pattern noise
+    FpnState fpn;
+
+    // post-process background
+    std::vector<float> bg_profile;
+    bool bg_record_requested = false;
+
+    // host-path buffers
+    void* d_in = nullptr;
+    float* d_out = nullptr;
+
+    // test hook: next launch skips its first bulk copy and waits at most this long
+    unsigned long long inject_stall_ns = 0;
+
+    std::string err;
+    std::mutex mu;
+};
+
+namespace {
+
+int fail(ope_b200_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(ope_b200_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, OPE_B200_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define OPE_CU(ctx, call)                                         \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
+    } while (0)
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int validate_cfg(const ope_b200_config* c, std::string* why) {
+    if (!c) { *why = "null configuration"; return OPE_B200_E_INVALID; }
+    if (c->signal_length <= 0 || c->ascans_per_bscan <= 0 || c->bscans_per_buffer <= 0) {
+        *why = "invalid processor configuration (non-positive dimension)";
+        return OPE_B200_E_INVALID;
+    }
+    if (!chain_length_supported(c->signal_length)) {
+        *why = "signal length " + std::to_string(c->signal_length) +
+               " unsupported: the B200 chain needs a power of two in [512, 8192]";
+        return OPE_B200_E_UNSUPPORTED;
+    }
+    if (input_kind(c->input_dtype, c->float32_as_uint32 != 0) < 0) {
+        *why = "input data type " + std::to_string(c->input_dtype) + " unsupported";
+        return OPE_B200_E_UNSUPPORTED;
+    }
+    if (c->resampling_enabled && (c->interpolation < 0 || c->interpolation > 2)) {
+        *why = "unknown interpolation method";
+        return OPE_B200_E_INVALID;
+    }
+    if (c->dc_removal_enabled && c->dc_window <= 0) {
+        *why = "rolling-average window must be >= 1";
+        return OPE_B200_E_INVALID;
+    }
+    if (c->fpn_bscan_count < 1) {
+        *why = "fixedPatternNoiseBscanCount must be >= 1";
+        return OPE_B200_E_INVALID;
+    }
+    return OPE_B200_OK;
+}
+
+void free_slot(TableSlot& s) {
+    cudaFree(s.lin);
+    cudaFree(s.cub);
+    cudaFree(s.lzb);
+    cudaFree(s.lzw);
+    cudaFree(s.wph);
+    if (s.last_use) cudaEventDestroy(s.last_use);
+    s = TableSlot{};
+}
+
+// Builds the device tables from the current curves into the inactive slot.
+int rebuild_tables(ope_b200_ctx* c) {
+    const int n = c->n;
+    const auto& cfg = c->cfg;
+    const int target = (c->active == 0) ? 1 : 0;
+    TableSlot& s = c->slot[target];
+    OPE_CU(c, cudaEventSynchronize(s.last_use));  // no in-flight launch still reads this slot
+
+    // resampling
+    c->interp = INTERP_NONE;
+    if (cfg.resampling_enabled) {
+        if (c->resample.size() != static_cast<size_t>(n))
+            return fail(c, OPE_B200_E_STATE, "resampling enabled but no curve of length N was set");
+        const int method = cfg.interpolation;
+        if (method == 0) {
+            std::vector<int2> tab = build_linear_table(c->resample.data(), n);
+            OPE_CU(c, cudaMemcpy(s.lin, tab.data(), n * sizeof(int2), cudaMemcpyHostToDevice));
+            c->interp = INTERP_LINEAR;
+        } else if (method == 1) {
+            std::vector<int4> tab = build_cubic_table(c->resample.data(), n);
+            OPE_CU(c, cudaMemcpy(s.cub, tab.data(), n * sizeof(int4), cudaMemcpyHostToDevice));
+            c->interp = INTERP_CUBIC;
+        } else {
+            std::vector<int> base;
+            std::vector<float> w;
+            build_lanczos_table(c->resample.data(), n, base, w);
+            OPE_CU(c, cudaMemcpy(s.lzb, base.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+            OPE_CU(c, cudaMemcpy(s.lzw, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+            c->interp = INTERP_LANCZOS;
+        }
+    }
+
+    // window x phase: a disabled stage multiplies by exactly 1 (cos 1, sin 0)
+    const bool win = cfg.windowing_enabled && c->window.size() == static_cast<size_t>(n);
+    if (cfg.windowing_enabled && !win)
+        return fail(c, OPE_B200_E_STATE, "windowing enabled but no window curve of length N was set");
+    // dispersionCompensation skips when the phase length differs from N (cpu_kernels.tpp:205-208)
+    const bool disp = cfg.dispersion_enabled && c->cos_sin.size() == 2 * static_cast<size_t>(n);
+    std::vector<float4> wph = build_window_phase(win ? c->window.data() : nullptr, disp ? c->cos_sin.data() : nullptr, n);
+    OPE_CU(c, cudaMemcpy(s.wph, wph.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    c->active = target;
+    c->tables_dirty = false;
+    return OPE_B200_OK;
+}
+
+int alloc_slot(ope_b200_ctx* c, TableSlot& s) {
+    const size_t n = static_cast<size_t>(c->n);
+    OPE_CU(c, cudaMalloc(&s.lin, n * sizeof(int2)));
+    OPE_CU(c, cudaMalloc(&s.cub, n * sizeof(int4)));
+    OPE_CU(c, cudaMalloc(&s.lzb, n * sizeof(int)));
+    OPE_CU(c, cudaMalloc(&s.lzw, 16 * n * sizeof(float)));
+    OPE_CU(c, cudaMalloc(&s.wph, n * sizeof(float4)));
+    OPE_CU(c, cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
+    return OPE_B200_OK;
+}
+
+}  // namespace
+
+namespace ope_b200 {
+bool chain_length_supported(int n) { return n >= 512 && n <= 8192 && (n & (n - 1)) == 0; }
+}  // namespace ope_b200
+
+// Builds kernel arguments for the current configuration; tables must be valid.
+static ChainArgs make_args(ope_b200_ctx* c, const void* d_in, float* d_out, long long m, const float2* fpn) {
+    ChainArgs a{};
+    a.in = d_in;
+    a.out = d_out;
+    a.m = m;
+    a.tw = c->d_tw;
+    const TableSlot& s = c->slot[c->active];
+    a.lin = s.lin;
+    a.cub = s.cub;
+    a.lz_base = s.lzb;
+    a.lz_w = s.lzw;
+    a.wph = s.wph;
+    a.fpn = fpn;
+    a.dc_window = c->cfg.dc_removal_enabled ? c->cfg.dc_window : 0;
+    const auto& cf = c->cfg;
+    scaling_constants(cf.log_scaling != 0, cf.grayscale_min, cf.grayscale_max, cf.addend, cf.multiplicator, c->n, a);
+    a.flip = c->cfg.bscan_flip ? 1 : 0;
+    a.ascans_per_bscan = c->cfg.ascans_per_bscan;
+    a.bscans = static_cast<int>((m + c->cfg.ascans_per_bscan - 1) / c->cfg.ascans_per_bscan);
+    a.status = c->d_status;
+    a.timeout_ns = 2000000000ull;
+    return a;
+}
+
+extern "C" {
+
+int ope_b200_abi_version(void) { return OPE_B200_ABI_VERSION; }
+
+int ope_b200_device_supported(int32_t device) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return 0;
+    return p.major == 10 ? 1 : 0;
+}
+
+void ope_b200_config_default(ope_b200_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->signal_length = 1024;
+    c->ascans_per_bscan = 512;
+    c->bscans_per_buffer = 1;
+    c->input_dtype = DT_UINT16;
+    c->interpolation = 0;
+    c->dc_window = 64;
+    c->log_scaling = 1;
+    c->grayscale_min = 30.0f;
+    c->grayscale_max = 100.0f;
+    c->addend = 0.0f;
+    c->multiplicator = 1.0f;
+    c->fpn_bscan_count = 1;
+    c->bg_weight = 1.0f;
+    c->bg_offset = 0.0f;
+    c->num_input_buffers = 2;
+}
+
+int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out) {
+    if (!out) return OPE_B200_E_INVALID;
+    *out = nullptr;
+    std::string why;
+    int rc = validate_cfg(cfg, &why);
+    if (rc != OPE_B200_OK) {
+        std::fprintf(stderr, "ope_b200_create: %s\n", why.c_str());
+        return rc;
+    }
+    auto* c = new ope_b200_ctx();
+    c->cfg = *cfg;
+    c->n = cfg->signal_length;
+    c->m = static_cast<long long>(cfg->ascans_per_bscan) * cfg->bscans_per_buffer;
+    c->in_kind = input_kind(cfg->input_dtype, cfg->float32_as_uint32 != 0);
+    c->in_bytes = static_cast<size_t>(c->m) * c->n * bytes_of(cfg->input_dtype);
+    c->out_bytes = static_cast<size_t>(c->m) * (c->n / 2) * sizeof(float);
+    c->device = cfg->device;
+    auto bail = [&](int code) {
+        ope_b200_destroy(c);
+        return code;
+    };
+    if (cudaSetDevice(c->device) != cudaSuccess) return bail(OPE_B200_E_CUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(OPE_B200_E_CUDA);
+    for (auto& s : c->slot)
+        if (alloc_slot(c, s) != OPE_B200_OK) return bail(OPE_B200_E_CUDA);
+    std::vector<float2> tw = build_twiddles(c->n);
+    if (cudaMalloc(&c->d_tw, c->n * sizeof(float2)) != cudaSuccess) return bail(OPE_B200_E_NOMEM);
+    if (cudaMemcpy(c->d_tw, tw.data(), c->n * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(OPE_B200_E_CUDA);
+    if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) return bail(OPE_B200_E_NOMEM);
+    if (cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) return bail(OPE_B200_E_CUDA);
+    if (fpn_init(c->fpn, c->n) != cudaSuccess) return bail(OPE_B200_E_NOMEM);
+    *out = c;
+    return OPE_B200_OK;
+}
+
+void ope_b200_destroy(ope_b200_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& s : c->slot) free_slot(s);
+    cudaFree(c->d_tw);
+    cudaFree(c->d_status);
+    cudaFree(c->d_in);
+    cudaFree(c->d_out);
+    fpn_free(c->fpn);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* ope_b200_last_error(const ope_b200_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int ope_b200_update_config(ope_b200_ctx* c, const ope_b200_config* cfg) {
+    if (!c || !cfg) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    std::string why;
+    int rc = validate_cfg(cfg, &why);
+    if (rc != OPE_B200_OK) return fail(c, rc, why);
+    if (cfg->signal_length != c->cfg.signal_length || cfg->ascans_per_bscan != c->cfg.ascans_per_bscan ||
+        cfg->bscans_per_buffer != c->cfg.bscans_per_buffer || cfg->device != c->cfg.device)
+        return fail(c, OPE_B200_E_STATE, "dimension change requires a new context");
+    const bool dt_change = cfg->input_dtype != c->cfg.input_dtype || cfg->float32_as_uint32 != c->cfg.float32_as_uint32;
+    c->cfg = *cfg;
+    if (dt_change) {
+        c->in_kind = input_kind(cfg->input_dtype, cfg->float32_as_uint32 != 0);
+        c->in_bytes = static_cast<size_t>(c->m) * c->n * bytes_of(cfg->input_dtype);
+        cudaFree(c->d_in);
+        c->d_in = nullptr;
+    }
+    c->tables_dirty = true;
+    return OPE_B200_OK;
+}
+
+int ope_b200_set_resampling_curve(ope_b200_ctx* c, const float* curve, size_t n) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!curve && n > 0) return fail(c, OPE_B200_E_INVALID, "Invalid resampling curve pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resample.assign(curve, curve + n);
+    c->tables_dirty = true;
+    return OPE_B200_OK;
+}
+
+int ope_b200_set_window_curve(ope_b200_ctx* c, const float* curve, size_t n) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!curve && n > 0) return fail(c, OPE_B200_E_INVALID, "Invalid window curve pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->window.assign(curve, curve + n);
+    c->tables_dirty = true;
+    return OPE_B200_OK;
+}
+
+int ope_b200_set_dispersion_curve(ope_b200_ctx* c, const float* cs, size_t n_floats) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!cs && n_floats > 0) return fail(c, OPE_B200_E_INVALID, "Invalid dispersion curve pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->cos_sin.assign(cs, cs + (n_floats / 2) * 2);
+    c->tables_dirty = true;
+    return OPE_B200_OK;
+}
+
+static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long long m, cudaStream_t s,
+                          bool bins = false) {
+    if (!d_in || !d_out || m < 1) return fail(c, OPE_B200_E_INVALID, "null buffer or empty A-scan count");
+    if (!aligned16(d_in)) return fail(c, OPE_B200_E_INVALID, "input buffer must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(d_out) & (bins ? 7u : 3u)) != 0)
+        return fail(c, OPE_B200_E_INVALID, "output buffer is not aligned to its element size");
+    OPE_CU(c, cudaSetDevice(c->device));
+    if (c->tables_dirty) {
+        int rc = rebuild_tables(c);
+        if (rc != OPE_B200_OK) return rc;
+    }
+    // fixed-pattern noise: determination (statistics pass + finalize) before
+    // the frame that uses it, as computeFixedPatternNoiseIfRequested runs
+    // before the subtraction loop (cpu_backend.cpp:245-255)
+    const float2* fpn = nullptr;
+    if (c->cfg.fpn_removal || c->fpn.requested || c->cfg.fpn_continuous) {
+        ChainArgs a = make_args(c, d_in, nullptr, m, nullptr);
+        int rc = fpn_process_frame(c->fpn, c->cfg, c->in_kind, c->interp, a, s, &c->err);
+        if (rc != OPE_B200_OK) return rc;
+        if (c->cfg.fpn_removal && c->fpn.valid) fpn = c->fpn.d_profile;
+    }
+    ChainArgs a = make_args(c, d_in, bins ? nullptr : static_cast<float*>(d_out), m, fpn);
+    if (bins) a.bins_out = static_cast<float2*>(d_out);
+    if (c->inject_stall_ns) {
+        a.debug_skip_first_copy = 1;
+        a.timeout_ns = c->inject_stall_ns;
+        c->inject_stall_ns = 0;
+    }
+    cudaError_t e = launch_chain(c->n, c->in_kind, c->interp, a, s, 0, nullptr);
+    if (e != cudaSuccess) return cuda_fail(c, e, "chain launch");
+    OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
+    return OPE_B200_OK;
+}
+
+int ope_b200_process_device_n(ope_b200_ctx* c, const void* d_in, float* d_out, int64_t m, void* stream) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return process_locked(c, d_in, d_out, m, static_cast<cudaStream_t>(stream));
+}
+
+int ope_b200_process_bins_device(ope_b200_ctx* c, const void* d_in, void* d_bins, int64_t m, void* stream) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return process_locked(c, d_in, d_bins, m, static_cast<cudaStream_t>(stream), true);
+}
+
+int ope_b200_test_inject_copy_stall(ope_b200_ctx* c, uint32_t timeout_us) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->inject_stall_ns = static_cast<unsigned long long>(timeout_us ? timeout_us : 1) * 1000ull;
+    return OPE_B200_OK;
+}
+
+int ope_b200_process_device(ope_b200_ctx* c, const void* d_in, float* d_out, void* stream) {
+    if (!c) return OPE_B200_E_INVALID;
+    return ope_b200_process_device_n(c, d_in, d_out, c->m, stream);
+}
+
+int ope_b200_process_host(ope_b200_ctx* c, const void* h_in, float* h_out) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!h_in || !h_out) return fail(c, OPE_B200_E_INVALID, "null host buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    if (!c->d_in) OPE_CU(c, cudaMalloc(&c->d_in, c->in_bytes));
+    if (!c->d_out) OPE_CU(c, cudaMalloc(&c->d_out, c->out_bytes));
+    OPE_CU(c, cudaMemcpyAsync(c->d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, c->stream));
+    int rc = process_locked(c, c->d_in, c->d_out, c->m, c->stream);
+    if (rc != OPE_B200_OK) return rc;
+    OPE_CU(c, cudaMemcpyAsync(h_out, c->d_out, c->out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    OPE_CU(c, cudaStreamSynchronize(c->stream));
+    int st = 0;
+    OPE_CU(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0) {
+        cudaMemset(c->d_status, 0, sizeof(int));
+        return fail(c, OPE_B200_E_DEVICE, "kernel reported status " + std::to_string(st));
+    }
+    return OPE_B200_OK;
+}
+
+int ope_b200_synchronize(ope_b200_ctx* c, int32_t* device_status) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    OPE_CU(c, cudaDeviceSynchronize());
+    int st = 0;
+    OPE_CU(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    OPE_CU(c, cudaMemset(c->d_status, 0, sizeof(int)));
+    if (device_status) *device_status = st;
+    return OPE_B200_OK;
+}
+
+int ope_b200_request_fpn_determination(ope_b200_ctx* c) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->fpn.requested = true;
+    return OPE_B200_OK;
+}
+
+int ope_b200_set_fpn_profile(ope_b200_ctx* c, const float* p, size_t pairs) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!p && pairs > 0) return fail(c, OPE_B200_E_INVALID, "Invalid fixed-pattern noise profile pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    return fpn_set_profile(c->fpn, p, pairs, c->stream, &c->err);
+}
+
+int ope_b200_get_fpn_profile(ope_b200_ctx* c, float* out, size_t cap_pairs, size_t* pairs) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    return fpn_get_profile(c->fpn, out, cap_pairs, pairs, &c->err);
+}
+
+int ope_b200_request_bg_recording(ope_b200_ctx* c) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->bg_record_requested = true;
+    return fail(c, OPE_B200_E_UNSUPPORTED, "post-process background recording is not implemented yet");
+}
+
+int ope_b200_set_bg_profile(ope_b200_ctx* c, const float* p, size_t n) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!p) return fail(c, OPE_B200_E_INVALID, "Background curve data is null");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (n != static_cast<size_t>(c->n / 2))
+        return fail(c, OPE_B200_E_INVALID, "Invalid background buffer size. Expected " + std::to_string(c->n / 2) +
+                                               " but got " + std::to_string(n));
+    c->bg_profile.assign(p, p + n);
+    return OPE_B200_OK;
+}
+
+int ope_b200_get_bg_profile(ope_b200_ctx* c, float* out, size_t cap, size_t* n) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (n) *n = c->bg_profile.size();
+    if (out) std::memcpy(out, c->bg_profile.data(), std::min(cap, c->bg_profile.size()) * sizeof(float));
+    return OPE_B200_OK;
+}
+
+}  // extern "C"
+
+namespace ope_b200 {
+
+cudaError_t launch_chain(int n, int in_kind, int interp, const ChainArgs& a, cudaStream_t s, int max_ctas,
+                         LaunchInfo* info) {
+    switch (n) {
+        case 512: return launch_chain_n512(in_kind, interp, a, s, max_ctas, info);
+        case 1024: return launch_chain_n1024(in_kind, interp, a, s, max_ctas, info);
+        case 2048: return launch_chain_n2048(in_kind, interp, a, s, max_ctas, info);
+        case 4096: return launch_chain_n4096(in_kind, interp, a, s, max_ctas, info);
+        case 8192: return launch_chain_n8192(in_kind, interp, a, s, max_ctas, info);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ope_b200

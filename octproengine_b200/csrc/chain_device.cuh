@@ -1,0 +1,390 @@
+// Device-only parts of the fused chain: TMA bulk copies, bounded mbarrier
+// waits, team reductions and the persistent __global__ kernel.
+#pragma once
+
+#include "chain_kernel.cuh"
+
+namespace ope_b200 {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Non-multicast 1-D bulk copy global -> this CTA's shared memory, completing
+// `bytes` of transaction count on `bar`. Source and destination must be
+// 16-byte aligned and `bytes` a multiple of 16 (checked by the host).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of `bar`, giving up after timeout_ns.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned long long timeout_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (global_ns() - t0 > timeout_ns) return false;
+    }
+    return true;
+}
+
+// Exclusive team scan of two values per thread (T threads, T % 32 == 0).
+template <int T, typename S>
+__device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    S ia = a, ib = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        S xa = __shfl_up_sync(0xffffffffu, ia, o);
+        S xb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= o) {
+            ia += xa;
+            ib += xb;
+        }
+    }
+    if (lane == 31) {
+        scratch[2 * warp] = ia;
+        scratch[2 * warp + 1] = ib;
+    }
+    __syncthreads();
+    S pa = 0, pb = 0;
+    for (int w = 0; w < warp; ++w) {
+        pa += scratch[2 * w];
+        pb += scratch[2 * w + 1];
+    }
+    a = pa + ia - a;
+    b = pb + ib - b;
+}
+
+template <int T>
+__device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn.x = fminf(mn.x, __shfl_xor_sync(0xffffffffu, mn.x, o));
+        mn.y = fminf(mn.y, __shfl_xor_sync(0xffffffffu, mn.y, o));
+        mx.x = fmaxf(mx.x, __shfl_xor_sync(0xffffffffu, mx.x, o));
+        mx.y = fmaxf(mx.y, __shfl_xor_sync(0xffffffffu, mx.y, o));
+    }
+    if (lane == 0) {
+        scratch[4 * warp + 0] = mn.x;
+        scratch[4 * warp + 1] = mn.y;
+        scratch[4 * warp + 2] = mx.x;
+        scratch[4 * warp + 3] = mx.y;
+    }
+    __syncthreads();
+    mn = make_float2(scratch[0], scratch[1]);
+    mx = make_float2(scratch[2], scratch[3]);
+    for (int w = 1; w < T / 32; ++w) {
+        mn.x = fminf(mn.x, scratch[4 * w + 0]);
+        mn.y = fminf(mn.y, scratch[4 * w + 1]);
+        mx.x = fmaxf(mx.x, scratch[4 * w + 2]);
+        mx.y = fmaxf(mx.y, scratch[4 * w + 3]);
+    }
+}
+
+// Output stage for one pair: scaling, affine map, streaming stores.
+template <int N>
+__device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a, long long row_a, float* scratch) {
+    using L = LastInfo<N>;
+    constexpr int NB = L::NB;
+    float2 mag2[NB];
+    epi_mag2<N>(t, v, a, mag2);
+    float2 res[NB];
+    if (a.log_mode) {
+#pragma unroll
+        for (int k = 0; k < NB; ++k) res[k] = make_float2(fast_log2(mag2[k].x), fast_log2(mag2[k].y));
+        if (a.auto_minmax) {
+            // logScaleAndTruncate auto range (cpu_kernels.tpp:327-335): per A-scan
+            // min/max of 10*log10(|X|^2/(N/2)) over the kept bins.
+            const float c10 = 3.01029995663981195214f;  // 10*log10(2)
+            const float off = c10 * (float)Plan<N>::LOG2N - c10;  // 10*log10(N/2)
+            float2 mn = make_float2(INFINITY, INFINITY), mx = make_float2(-INFINITY, -INFINITY);
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                res[k] = make_float2(fmaf(c10, res[k].x, -off), fmaf(c10, res[k].y, -off));
+                mn = make_float2(fminf(mn.x, res[k].x), fminf(mn.y, res[k].y));
+                mx = make_float2(fmaxf(mx.x, res[k].x), fmaxf(mx.y, res[k].y));
+            }
+            team_minmax2<Plan<N>::T>(mn, mx, scratch);
+            float ra = mx.x - mn.x, rb = mx.y - mn.y;
+            if (!(ra >= 1e-6f)) ra = 1.0f;
+            if (!(rb >= 1e-6f)) rb = 1.0f;
+            const float sa = a.mult / ra, sb = a.mult / rb;
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                res[k] = make_float2(fmaf(sa, res[k].x - mn.x, a.mult * a.addend),
+                                     fmaf(sb, res[k].y - mn.y, a.mult * a.addend));
+        } else {
+#pragma unroll
+            for (int k = 0; k < NB; ++k) res[k] = fma2(res[k], dup2(a.k_a), dup2(a.k_b));
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+            res[k] = fma2(make_float2(fsqrt(mag2[k].x), fsqrt(mag2[k].y)), dup2(a.k_a), dup2(a.k_b));
+    }
+    const long long oa = out_row(a, row_a) * (long long)(N / 2);
+    const bool has_b = row_a + 1 < a.m;
+    const long long ob = has_b ? out_row(a, row_a + 1) * (long long)(N / 2) : 0;
+#pragma unroll
+    for (int i = 0; i < L::D; ++i)
+#pragma unroll
+        for (int q = 0; q < L::R / 2; ++q) {
+            const int bin = L::bin(t, i, q);
+            const float2 r = res[i * (L::R / 2) + q];
+            __stcs(a.out + oa + bin, r.x);
+            if (has_b) __stcs(a.out + ob + bin, r.y);
+        }
+}
+
+// Runs the chain up to the last FFT pass for the pairs p = p0, p0 + step, ...
+// (< p_end) whose rows are row0 + 2p and row0 + 2p + 1 (the second one only if
+// < row_end), and hands each pair's bins to `sink(t, v, row_a, has_b)`.
+// Raw rows are staged by cp.async.bulk into a two-deep ring; every wait is
+// bounded (a.timeout_ns) and a timeout sets STATUS_MBAR_TIMEOUT and returns.
+template <int N, int DT, int INTERP, class Sink>
+__device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, long long row_end, long long p0,
+                                          long long p_end, long long step, unsigned char* smem, Sink& sink) {
+    using PL = Plan<N>;
+    using LY = Layout<N, DT>;
+    using sum_t = typename InTraits<DT>::sum_t;
+    using raw_t = typename InTraits<DT>::raw_t;
+    constexpr int T = PL::T;
+    constexpr int NPASS = PL::NPASS;
+
+    float2* spec = reinterpret_cast<float2*>(smem + LY::OFF_SPEC);
+    float4* exch = reinterpret_cast<float4*>(smem + LY::OFF_EXCH);
+    sum_t* pfx = reinterpret_cast<sum_t*>(smem + LY::OFF_PFX);
+    sum_t* scan = reinterpret_cast<sum_t*>(smem + LY::OFF_SCAN);
+    unsigned char* stages = smem + LY::OFF_STAGE;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + LY::OFF_MBAR);
+    int* abort_flag = reinterpret_cast<int*>(smem + LY::OFF_MBAR + 16);
+
+    const int t = threadIdx.x;
+    constexpr uint32_t ROW_BYTES = N * sizeof(raw_t);
+    const unsigned char* in = static_cast<const unsigned char*>(a.in);
+
+    if (t == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+        *abort_flag = 0;
+    }
+    __syncthreads();
+
+    auto issue = [&](long long pair, int st) {
+        const long long r = row0 + 2 * pair;
+        const uint32_t rows = (row_end - r) >= 2 ? 2u : 1u;
+        const uint32_t bytes = rows * ROW_BYTES;
+        fence_proxy_async_smem();
+        mbar_expect_tx(&mbar[st], bytes);
+        bulk_g2s(stages + st * LY::STAGE_BYTES, in + r * (long long)ROW_BYTES, bytes, &mbar[st]);
+    };
+
+    long long item = p0;
+    if (t == 0 && item < p_end && !a.debug_skip_first_copy) issue(item, 0);
+
+    for (int it = 0; item < p_end; item += step, ++it) {
+        const int st = it & 1;
+        const long long nxt = item + step;
+        if (t == 0 && nxt < p_end) issue(nxt, st ^ 1);
+        if (!mbar_wait_bounded(&mbar[st], (it >> 1) & 1, a.timeout_ns)) *abort_flag = 1;
+        __syncthreads();
+        if (*abort_flag) {
+            if (t == 0) {
+                if (a.status) atomicOr(a.status, STATUS_MBAR_TIMEOUT);
+                if (nxt < p_end) (void)mbar_wait_bounded(&mbar[st ^ 1], ((it + 1) >> 1) & 1, a.timeout_ns);
+            }
+            return;
+        }
+        const unsigned char* stage = stages + st * LY::STAGE_BYTES;
+
+        // ---- unpack (+ DC removal) ----
+        if (a.dc_window > 0) {
+            sum_t ta, tb;
+            phase_dc_local<N, DT>(t, stage, &ta, &tb);
+            team_exclusive_scan2<T, sum_t>(ta, tb, scan);
+            phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
+            __syncthreads();
+            phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
+        } else {
+            phase_unpack<N, DT>(t, stage, spec);
+        }
+        __syncthreads();
+
+        // ---- k-linearisation, window, phase; pass 0 ----
+        cp v[16];
+        phase_prestage<N, INTERP>(t, spec, a, v);
+        fft_twiddle_dft<N, 0>(t, v, a.tw);
+        __syncthreads();  // spec aliases the exchange buffer
+        fft_store<N, 0>(t, v, exch);
+        __syncthreads();
+        if constexpr (NPASS > 2) {
+            fft_load<N>(t, exch, v);
+            fft_twiddle_dft<N, 1>(t, v, a.tw);
+            __syncthreads();
+            fft_store<N, 1>(t, v, exch);
+            __syncthreads();
+        }
+        if constexpr (NPASS > 3) {
+            fft_load<N>(t, exch, v);
+            fft_twiddle_dft<N, 2>(t, v, a.tw);
+            __syncthreads();
+            fft_store<N, 2>(t, v, exch);
+            __syncthreads();
+        }
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, NPASS - 1>(t, v, a.tw);
+        const long long ra = row0 + 2 * item;
+        sink(t, v, ra, ra + 1 < row_end);
+        __syncthreads();  // next item overwrites spec/exch
+    }
+}
+
+template <int N>
+struct ImageSink {
+    const ChainArgs& a;
+    float* scratch;
+    __device__ __forceinline__ void operator()(int t, const cp* v, long long row_a, bool has_b) {
+        if (a.bins_out) {
+            // complex bins after the (optional) FPN subtraction, before magnitude
+            using L = LastInfo<N>;
+#pragma unroll
+            for (int i = 0; i < L::D; ++i)
+#pragma unroll
+                for (int q = 0; q < L::R / 2; ++q) {
+                    const int bin = L::bin(t, i, q);
+                    cp x = v[i + q * L::D];
+                    if (a.fpn) {
+                        const float2 f = __ldg(a.fpn + bin);
+                        x.re = sub2(x.re, dup2(f.x));
+                        x.im = sub2(x.im, dup2(f.y));
+                    }
+                    a.bins_out[row_a * (N / 2) + bin] = make_float2(x.re.x, x.im.x);
+                    if (has_b) a.bins_out[(row_a + 1) * (N / 2) + bin] = make_float2(x.re.y, x.im.y);
+                }
+            return;
+        }
+        epilogue<N>(t, v, a, row_a, scratch);
+    }
+};
+
+template <int N, int DT, int INTERP>
+__global__ void __launch_bounds__(N / 16) chain_kernel(const ChainArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    using LY = Layout<N, DT>;
+    ImageSink<N> sink{a, reinterpret_cast<float*>(smem + LY::OFF_SCAN)};
+    const long long npairs = (a.m + 1) / 2;
+    run_pairs<N, DT, INTERP>(a, 0, a.m, blockIdx.x, npairs, gridDim.x, smem, sink);
+}
+
+}  // namespace ope_b200
+
+namespace ope_b200 {
+
+// Accumulates, per kept bin, sum re, sum im and sum |z|^2 (double) over the
+// A-scans this CTA processes; the minimum-variance mean of
+// getMinimumVarianceMean (cpu_kernels.tpp:402-458) is built from these sums.
+template <int N>
+struct FpnStatsSink {
+    using L = LastInfo<N>;
+    double acc[L::NB][3];
+    const float2* fpn_unused;
+    __device__ __forceinline__ void reset() {
+#pragma unroll
+        for (int k = 0; k < L::NB; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    }
+    __device__ __forceinline__ void operator()(int, const cp* v, long long, bool has_b) {
+#pragma unroll
+        for (int i = 0; i < L::D; ++i)
+#pragma unroll
+            for (int q = 0; q < L::R / 2; ++q) {
+                const cp x = v[i + q * L::D];
+                const int k = i * (L::R / 2) + q;
+                double re = x.re.x, im = x.im.x;
+                acc[k][0] += re;
+                acc[k][1] += im;
+                acc[k][2] += re * re + im * im;
+                if (has_b) {
+                    re = x.re.y;
+                    im = x.im.y;
+                    acc[k][0] += re;
+                    acc[k][1] += im;
+                    acc[k][2] += re * re + im * im;
+                }
+            }
+    }
+};
+
+// grid = (gx, 8): blockIdx.y is the FPN segment. Segment s covers accumulation
+// rows [s*seg_w, (s+1)*seg_w); this buffer holds accumulation rows
+// [g0, g0 + rows). Partials: partial[((s*gx + bx)*(N/2) + bin)*3 + k].
+template <int N, int DT, int INTERP>
+__global__ void __launch_bounds__(N / 16) fpn_stats_kernel(const ChainArgs a, long long g0, long long rows,
+                                                             long long seg_w, double* partial) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    using L = LastInfo<N>;
+    const int s = blockIdx.y;
+    const long long glo = (long long)s * seg_w, ghi = glo + seg_w;
+    long long lo = (glo > g0 ? glo : g0) - g0;
+    long long hi = (ghi < g0 + rows ? ghi : g0 + rows) - g0;
+    FpnStatsSink<N> sink;
+    sink.reset();
+    if (hi > lo) {
+        const long long npairs = (hi - lo + 1) / 2;
+        run_pairs<N, DT, INTERP>(a, lo, hi, blockIdx.x, npairs, gridDim.x, smem, sink);
+    }
+    const int t = threadIdx.x;
+    double* dst = partial + ((long long)s * gridDim.x + blockIdx.x) * (N / 2) * 3;
+#pragma unroll
+    for (int i = 0; i < L::D; ++i)
+#pragma unroll
+        for (int q = 0; q < L::R / 2; ++q) {
+            const int bin = L::bin(t, i, q);
+            const int k = i * (L::R / 2) + q;
+            dst[bin * 3 + 0] = sink.acc[k][0];
+            dst[bin * 3 + 1] = sink.acc[k][1];
+            dst[bin * 3 + 2] = sink.acc[k][2];
+        }
+}
+
+}  // namespace ope_b200

@@ -1,0 +1,512 @@
+// Fused per-A-scan OCT chain for B200 (sm_100a).
+//
+// One CTA ("team") of T = N/16 threads processes one PAIR of A-scans at a time
+// in a persistent loop; the two A-scans ride in the two lanes of packed f32x2
+// registers (pair_math.cuh). Per pair:
+//
+//   raw rows --(cp.async.bulk, double-buffered, mbarrier)--> smem
+//   unpack to float pairs (+ rolling-average DC removal)       -> smem "spec"
+//   k-linearisation gather (none / linear / cubic / Lanczos-8)  -> registers
+//   x window x (cos, sin) of the dispersion phase              -> registers
+//   inverse DFT: Stockham radix-16 passes through padded smem  -> registers
+//   FPN subtraction, |X|^2, log10 or linear scaling, affine    -> HBM (bins < N/2)
+//
+// Each raw spectrum is read from HBM once and each output once; everything in
+// between stays on chip. The stage semantics follow the reference CPU backend
+// (src/backends/cpu/cpu_kernels.tpp:24-378, cpu_backend.cpp:169-302); see the
+// notes at each phase.
+//
+// The phase functions are __host__ __device__ and take the thread index
+// explicitly, so the CPU emulation harness (tests/emu) runs this exact code
+// thread by thread between emulated barriers.
+#pragma once
+
+#include <cstring>
+
+#include "pair_math.cuh"
+
+#if !defined(__CUDACC__)
+#include <cassert>
+#define OPE_SMEM_CHECK(cond) assert(cond)
+#else
+#define OPE_SMEM_CHECK(cond) ((void)0)
+#endif
+
+namespace ope_b200 {
+
+// Input element types of the fused chain.
+enum InputKind : int { IN_U8 = 0, IN_U16 = 1, IN_U32 = 2, IN_F32 = 3 };
+// Resampling (k-linearisation) variants; the non-NONE values follow
+// ope::InterpolationMethod + 1 (include/processorconfiguration.h:16-20).
+enum InterpKind : int { INTERP_NONE = 0, INTERP_LINEAR = 1, INTERP_CUBIC = 2, INTERP_LANCZOS = 3 };
+
+// Replicated-edge padding of the unpacked spectrum: gathers at indices in
+// [-PAD, N+PAD) read the clamped edge value, which is how the reference clamps
+// (cpu_kernels.tpp:101-102,132-135,187-188).
+constexpr int SPEC_PAD = 16;
+
+// Device status word bits.
+constexpr int STATUS_MBAR_TIMEOUT = 1;
+
+struct ChainArgs {
+    const void* in;      // m rows x n samples
+    float* out;          // m rows x n/2 bins
+    long long m;         // A-scans in this buffer
+    const float2* tw;    // W_N^j = (cos, sin)(2 pi j / N), j < N
+    const int2* lin;     // LINEAR: {n1 + PAD, float bits of (nx - n1)}
+    const int4* cub;     // CUBIC: {n0|n1<<16, n2|n3<<16 (all +PAD), pos bits, pos^2 bits}
+    const int* lz_base;  // LANCZOS: first tap index + PAD
+    const float* lz_w;   // LANCZOS: 16 x N tap weights, tap-major
+    const float4* wph;   // {window, cos(phase), sin(phase), 0}
+    const float2* fpn;   // N/2 complex fixed-pattern profile, or nullptr
+    int dc_window;       // rolling-average half window W; 0 = off
+    int log_mode;        // 1: logarithmic, 0: linear
+    int auto_minmax;     // log mode with grayscaleMin == grayscaleMax
+    float k_a, k_b;      // log: out = k_a*log2|X|^2 + k_b; linear: out = k_a*|X| + k_b
+    float mult, addend;  // auto-minmax affine
+    int flip;            // B-scan flip (output row remap)
+    int ascans_per_bscan;
+    int bscans;          // B-scans in this buffer
+    int* status;         // device error word (may be nullptr)
+    unsigned long long timeout_ns;
+    float2* bins_out;    // if set: write complex bins [0, N/2) per A-scan instead of the image
+    int debug_skip_first_copy;  // test hook: never issue the first bulk copy (exercises the timeout path)
+};
+
+template <int N_>
+struct Plan {
+    static constexpr int N = N_;
+    static_assert(N >= 256 && N <= 8192 && (N & (N - 1)) == 0, "N must be a power of two in [256, 8192]");
+    static constexpr int T = N / 16;  // threads per team
+    static constexpr int LOG2N = (N == 256) ? 8 : (N == 512) ? 9 : (N == 1024) ? 10 : (N == 2048) ? 11 : (N == 4096) ? 12 : 13;
+    static constexpr int NPASS = (LOG2N + 3) / 4;
+    static constexpr int LASTR = 1 << (LOG2N - 4 * (NPASS - 1));
+    static constexpr int HALF = N / 2;
+    // padded exchange buffer: one float4 per element plus one per 16
+    static constexpr int EXCH_ELEMS = N + N / 16;
+};
+
+OPE_HD int xpad(int e) { return e + (e >> 4); }
+
+OPE_HD float bits_f(int b) {
+#if defined(__CUDA_ARCH__)
+    return __int_as_float(b);
+#else
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+
+template <int DT>
+struct InTraits;
+template <>
+struct InTraits<IN_U8> { using raw_t = unsigned char; using sum_t = int; };
+template <>
+struct InTraits<IN_U16> { using raw_t = unsigned short; using sum_t = int; };
+template <>
+struct InTraits<IN_U32> { using raw_t = unsigned int; using sum_t = long long; };
+template <>
+struct InTraits<IN_F32> { using raw_t = float; using sum_t = float; };
+
+// Shared-memory layout of one team (bytes).
+template <int N, int DT>
+struct Layout {
+    using sum_t = typename InTraits<DT>::sum_t;
+    using raw_t = typename InTraits<DT>::raw_t;
+    static constexpr int SPEC_BYTES = (N + 2 * SPEC_PAD) * 8;        // float2 pairs
+    static constexpr int PFX_BYTES = (N + 1) * 2 * (int)sizeof(sum_t);  // prefix sums, 2 rows
+    static constexpr int EXCH_BYTES_RAW = Plan<N>::EXCH_ELEMS * 16;
+    static constexpr int WORK_BYTES = (EXCH_BYTES_RAW > SPEC_BYTES + PFX_BYTES + 256)
+                                          ? EXCH_BYTES_RAW
+                                          : SPEC_BYTES + PFX_BYTES + 256;
+    static constexpr int STAGE_BYTES = 2 * N * (int)sizeof(raw_t);  // two raw rows
+    static constexpr int OFF_SPEC = 0;
+    static constexpr int OFF_PFX = SPEC_BYTES;
+    static constexpr int OFF_SCAN = SPEC_BYTES + PFX_BYTES;  // 256 B of scan scratch
+    static constexpr int OFF_EXCH = 0;
+    static constexpr int OFF_STAGE = ((WORK_BYTES + 127) / 128) * 128;
+    static constexpr int OFF_MBAR = OFF_STAGE + 2 * STAGE_BYTES;
+    static constexpr int TOTAL = OFF_MBAR + 64;
+};
+
+// ------------------------------------------------------------------ unpack --
+
+OPE_HD float u16_to_float(unsigned v) { return (float)v; }
+
+// Eight consecutive samples of both rows of a pair -> float pairs.
+template <int DT>
+OPE_HD void load_chunk8(const unsigned char* stage, int n, int c, float2* vals) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    const raw_t* ra = reinterpret_cast<const raw_t*>(stage);
+    const raw_t* rb = ra + n;
+#if defined(__CUDA_ARCH__)
+    if (DT == IN_U16) {
+        uint4 wa = *reinterpret_cast<const uint4*>(ra + 8 * c);
+        uint4 wb = *reinterpret_cast<const uint4*>(rb + 8 * c);
+        const unsigned wa4[4] = {wa.x, wa.y, wa.z, wa.w};
+        const unsigned wb4[4] = {wb.x, wb.y, wb.z, wb.w};
+        const float2 magic = dup2(8388608.0f);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // 0x4B00_0000 | u16 is the float 2^23 + u; subtracting 2^23 is exact.
+            float lo_a = __uint_as_float(__byte_perm(wa4[k], 0x4B00u, 0x5410));
+            float lo_b = __uint_as_float(__byte_perm(wb4[k], 0x4B00u, 0x5410));
+            float hi_a = __uint_as_float(__byte_perm(wa4[k], 0x4B00u, 0x5432));
+            float hi_b = __uint_as_float(__byte_perm(wb4[k], 0x4B00u, 0x5432));
+            vals[2 * k] = sub2(make_float2(lo_a, lo_b), magic);
+            vals[2 * k + 1] = sub2(make_float2(hi_a, hi_b), magic);
+        }
+        return;
+    }
+    if (DT == IN_U8) {
+        uint2 wa = *reinterpret_cast<const uint2*>(ra + 8 * c);
+        uint2 wb = *reinterpret_cast<const uint2*>(rb + 8 * c);
+        const unsigned wa2[2] = {wa.x, wa.y};
+        const unsigned wb2[2] = {wb.x, wb.y};
+        const float2 magic = dup2(8388608.0f);
+        const unsigned sel[4] = {0x5440, 0x5441, 0x5442, 0x5443};
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float a = __uint_as_float(__byte_perm(wa2[k], 0x4B00u, sel[j]));
+                float b = __uint_as_float(__byte_perm(wb2[k], 0x4B00u, sel[j]));
+                vals[4 * k + j] = sub2(make_float2(a, b), magic);
+            }
+        return;
+    }
+#endif
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        raw_t a = ra[8 * c + i];
+        raw_t b = rb[8 * c + i];
+        if (DT == IN_U32) {
+#if defined(__CUDA_ARCH__)
+            vals[i] = make_float2(__uint2float_rn((unsigned)a), __uint2float_rn((unsigned)b));
+#else
+            vals[i] = make_float2((float)(unsigned)a, (float)(unsigned)b);
+#endif
+        } else {
+            vals[i] = make_float2((float)a, (float)b);
+        }
+    }
+}
+
+template <int DT>
+OPE_HD void load_raw_pair(const unsigned char* stage, int n, int i, typename InTraits<DT>::sum_t& sa,
+                          typename InTraits<DT>::sum_t& sb) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    using sum_t = typename InTraits<DT>::sum_t;
+    const raw_t* ra = reinterpret_cast<const raw_t*>(stage);
+    sa = (sum_t)ra[i];
+    sb = (sum_t)ra[n + i];
+}
+
+// Plain unpack (no DC removal): spec[PAD + k] = (a[k], b[k]) for k < N, with
+// replicated edges. Thread t handles chunks c = t, t + T (8 samples each).
+template <int N, int DT>
+OPE_HD void phase_unpack(int t, const unsigned char* stage, float2* spec) {
+    constexpr int T = Plan<N>::T;
+#pragma unroll
+    for (int c = t; c < N / 8; c += T) {
+        float2 v[8];
+        load_chunk8<DT>(stage, N, c, v);
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            OPE_SMEM_CHECK(SPEC_PAD + 8 * c + i + 1 < N + 2 * SPEC_PAD);
+            *reinterpret_cast<float4*>(&spec[SPEC_PAD + 8 * c + i]) =
+                make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
+        }
+        if (c == 0) {
+            for (int k = 0; k < SPEC_PAD; ++k) spec[k] = v[0];
+        }
+        if (c == N / 8 - 1) {
+            for (int k = 0; k < SPEC_PAD; ++k) spec[SPEC_PAD + N + k] = v[7];
+        }
+    }
+}
+
+// Rolling-average DC removal (cpu_kernels.tpp:56-82): x[i] -= mean of
+// x[i-(W-1) .. min(i+W, N-1)]. Window sums come from exact integer prefix sums
+// (the reference accumulates them in float; for integer input whose running
+// sum stays below 2^24 both are identical).
+// Step A: thread t owns samples [16t, 16t+16); returns its two row totals.
+template <int N, int DT>
+OPE_HD void phase_dc_local(int t, const unsigned char* stage, typename InTraits<DT>::sum_t* tot_a,
+                           typename InTraits<DT>::sum_t* tot_b) {
+    using sum_t = typename InTraits<DT>::sum_t;
+    sum_t sa = 0, sb = 0;
+    for (int i = 16 * t; i < 16 * t + 16; ++i) {
+        sum_t a, b;
+        load_raw_pair<DT>(stage, N, i, a, b);
+        sa += a;
+        sb += b;
+    }
+    *tot_a = sa;
+    *tot_b = sb;
+}
+
+// Step B: with the exclusive prefix of the totals, write prefix sums
+// pfx[2*i + row] = sum_{k < i} x_row[k] for i in [16t, 16t+16] (pfx[0] = 0).
+template <int N, int DT>
+OPE_HD void phase_dc_prefix(int t, const unsigned char* stage, typename InTraits<DT>::sum_t ex_a,
+                            typename InTraits<DT>::sum_t ex_b, typename InTraits<DT>::sum_t* pfx) {
+    using sum_t = typename InTraits<DT>::sum_t;
+    sum_t sa = ex_a, sb = ex_b;
+    if (t == 0) {
+        pfx[0] = 0;
+        pfx[1] = 0;
+    }
+    for (int i = 16 * t; i < 16 * t + 16; ++i) {
+        sum_t a, b;
+        load_raw_pair<DT>(stage, N, i, a, b);
+        sa += a;
+        sb += b;
+        OPE_SMEM_CHECK(2 * (i + 1) + 1 < 2 * (N + 1));
+        pfx[2 * (i + 1)] = sa;
+        pfx[2 * (i + 1) + 1] = sb;
+    }
+}
+
+// Step C: subtract the window means and write the spectrum pairs.
+template <int N, int DT>
+OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InTraits<DT>::sum_t* pfx,
+                           int W, float2* spec) {
+    using sum_t = typename InTraits<DT>::sum_t;
+    constexpr int T = Plan<N>::T;
+#pragma unroll
+    for (int c = t; c < N / 8; c += T) {
+        float2 v[8];
+        load_chunk8<DT>(stage, N, c, v);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int i = 8 * c + k;
+            int start = (i >= W - 1) ? i - (W - 1) : 0;
+            int end = (i + W < N - 1) ? i + W : N - 1;
+            sum_t sa = pfx[2 * (end + 1)] - pfx[2 * start];
+            sum_t sb = pfx[2 * (end + 1) + 1] - pfx[2 * start + 1];
+            float cnt = (float)(end - start + 1);
+#if defined(__CUDA_ARCH__)
+            float ma = __fdiv_rn((float)sa, cnt);
+            float mb = __fdiv_rn((float)sb, cnt);
+#else
+            float ma = (float)sa / cnt;
+            float mb = (float)sb / cnt;
+#endif
+            v[k] = sub2(v[k], make_float2(ma, mb));
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i += 2)
+            *reinterpret_cast<float4*>(&spec[SPEC_PAD + 8 * c + i]) =
+                make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
+        if (c == 0)
+            for (int k = 0; k < SPEC_PAD; ++k) spec[k] = v[0];
+        if (c == N / 8 - 1)
+            for (int k = 0; k < SPEC_PAD; ++k) spec[SPEC_PAD + N + k] = v[7];
+    }
+}
+
+// ------------------------------------------------- resample, window, phase --
+// Produces the pass-0 inputs v[s] = z(t + s*T), s < 16.
+template <int N, int INTERP>
+OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v) {
+    constexpr int T = Plan<N>::T;
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+        const int j = t + s * T;
+        float2 y;
+        if (INTERP == INTERP_NONE) {
+            y = spec[SPEC_PAD + j];
+        } else if (INTERP == INTERP_LINEAR) {
+            // kLinearizationLinear (cpu_kernels.tpp:95-110): y1 + (y2 - y1) * (nx - n1)
+            int2 e = a.lin[j];
+            OPE_SMEM_CHECK(e.x >= 0 && e.x + 1 < N + 2 * SPEC_PAD);
+            float2 y1 = spec[e.x];
+            float2 y2 = spec[e.x + 1];
+            const float fr = bits_f(e.y);
+            y = add2(y1, mul2(sub2(y2, y1), dup2(fr)));
+        } else if (INTERP == INTERP_CUBIC) {
+            // kLinearizationCubic + cubicHermiteInterpolation (cpu_kernels.tpp:124-145,486-502)
+            int4 e = a.cub[j];
+            int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16, i2 = e.y & 0xFFFF, i3 = (unsigned)e.y >> 16;
+            OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 < N + 2 * SPEC_PAD && i2 < N + 2 * SPEC_PAD && i3 < N + 2 * SPEC_PAD);
+            const float pos = bits_f(e.z), pos2 = bits_f(e.w);
+            float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i2], y3 = spec[i3];
+            float2 ca = add2(sub2(mul2(dup2(3.0f), sub2(y1, y2)), y0), y3);
+            float2 cb = sub2(add2(sub2(mul2(dup2(2.0f), y0), mul2(dup2(5.0f), y1)), mul2(dup2(4.0f), y2)), y3);
+            float2 cc = sub2(y2, y0);
+            float2 in = add2(add2(mul2(ca, dup2(pos2)), mul2(cb, dup2(pos))), cc);
+            y = add2(mul2(dup2(fmul_rn(0.5f, pos)), in), y1);
+        } else {
+            // kLinearizationLanczos (cpu_kernels.tpp:176-195): sequential 16-tap sum
+            int b = a.lz_base[j];
+            OPE_SMEM_CHECK(b >= 0 && b + 15 < N + 2 * SPEC_PAD);
+            float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+#if defined(__CUDA_ARCH__)
+                float w = __ldg(a.lz_w + k * N + j);
+#else
+                float w = a.lz_w[k * N + j];
+#endif
+                acc = add2(acc, mul2(spec[b + k], dup2(w)));
+            }
+            y = acc;
+        }
+        // applyWindow then dispersionCompensation (cpu_kernels.tpp:198-235):
+        // re = (y*w)*cos, im = (y*w)*sin
+#if defined(__CUDA_ARCH__)
+        float4 q = __ldg(a.wph + j);
+#else
+        float4 q = a.wph[j];
+#endif
+        float2 yw = mul2(y, dup2(q.x));
+        v[s] = cpmake(mul2(yw, dup2(q.y)), mul2(yw, dup2(q.z)));
+    }
+}
+
+// ------------------------------------------------------------- FFT passes --
+// Stockham pass p with radix R = 16 (or LASTR for the last pass), Ns = 16^p:
+// DFT d = t + i*T (i < D = 16/R) reads x[d + r*N/R] = slot s = i + r*D,
+// multiplies by W_{Ns R}^{r k} (k = d mod Ns), and writes output q to
+// (d - k)*R + k + q*Ns.
+
+template <int N, int P>
+struct PassInfo {
+    static constexpr int NPASS = Plan<N>::NPASS;
+    static constexpr bool LAST = (P == NPASS - 1);
+    static constexpr int R = LAST ? Plan<N>::LASTR : 16;
+    static constexpr int D = 16 / R;
+    static constexpr int NS = (P == 0) ? 1 : (P == 1) ? 16 : (P == 2) ? 256 : 4096;
+};
+
+template <int N>
+OPE_HD void fft_load(int t, const float4* exch, cp* v) {
+    constexpr int T = Plan<N>::T;
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+        int e = t + s * T;
+        OPE_SMEM_CHECK(xpad(e) < Plan<N>::EXCH_ELEMS);
+        float4 q = exch[xpad(e)];
+        v[s] = cpmake(make_float2(q.x, q.y), make_float2(q.z, q.w));
+    }
+}
+
+template <int N, int P>
+OPE_HD void fft_twiddle_dft(int t, cp* v, const float2* tw) {
+    using PI = PassInfo<N, P>;
+    constexpr int T = Plan<N>::T;
+    constexpr int R = PI::R, D = PI::D, NS = PI::NS;
+    constexpr int NOUT = PI::LAST ? R / 2 : R;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        cp u[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = v[i + r * D];
+        if (P > 0) {
+            const int d = t + i * T;
+            const int k = d % NS;
+            const int stride = N / (NS * R);
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const int idx = r * k * stride;
+                OPE_SMEM_CHECK(idx >= 0 && idx < N);
+#if defined(__CUDA_ARCH__)
+                float2 w = __ldg(tw + idx);
+#else
+                float2 w = tw[idx];
+#endif
+                u[r] = cmul_tw(u[r], w.x, w.y);
+            }
+        }
+        if (R == 16) dft16<NOUT>(u);
+        else if (R == 8) dft8<NOUT>(u);
+        else if (R == 4) dft4v<NOUT>(u);
+        else dft2<NOUT>(u);
+#pragma unroll
+        for (int q = 0; q < NOUT; ++q) v[i + q * D] = u[q];
+    }
+}
+
+template <int N, int P>
+OPE_HD void fft_store(int t, const cp* v, float4* exch) {
+    using PI = PassInfo<N, P>;
+    constexpr int T = Plan<N>::T;
+    constexpr int R = PI::R, D = PI::D, NS = PI::NS;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        const int d = t + i * T;
+        const int k = d % NS;
+        const int base = (d - k) * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            int e = base + q * NS;
+            OPE_SMEM_CHECK(e >= 0 && e < N && xpad(e) < Plan<N>::EXCH_ELEMS);
+            cp x = v[i + q * D];
+            exch[xpad(e)] = make_float4(x.re.x, x.re.y, x.im.x, x.im.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- epilogue --
+OPE_HD float fast_log2(float x) {
+#if defined(__CUDA_ARCH__)
+    return __log2f(x);
+#else
+    return std::log2(x);
+#endif
+}
+OPE_HD float fsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+    return __fsqrt_rn(x);
+#else
+    return std::sqrt(x);
+#endif
+}
+
+// Bin b of the last pass lives in v[i + q*D] for b = (t + i*T) + q*N/R.
+template <int N>
+struct LastInfo {
+    using PI = PassInfo<N, Plan<N>::NPASS - 1>;
+    static constexpr int R = PI::R, D = PI::D;
+    static constexpr int NB = D * (R / 2);  // bins per thread
+    OPE_HD static int bin(int t, int i, int q) { return t + i * Plan<N>::T + q * (N / R); }
+};
+
+// |X|^2 with the optional fixed-pattern subtraction (cpu_kernels.tpp:460-479).
+template <int N>
+OPE_HD void epi_mag2(int t, const cp* v, const ChainArgs& a, float2* mag2) {
+    using L = LastInfo<N>;
+#pragma unroll
+    for (int i = 0; i < L::D; ++i)
+#pragma unroll
+        for (int q = 0; q < L::R / 2; ++q) {
+            cp x = v[i + q * L::D];
+            if (a.fpn) {
+                int b = L::bin(t, i, q);
+#if defined(__CUDA_ARCH__)
+                float2 f = __ldg(a.fpn + b);
+#else
+                float2 f = a.fpn[b];
+#endif
+                x.re = sub2(x.re, dup2(f.x));
+                x.im = sub2(x.im, dup2(f.y));
+            }
+            mag2[i * (L::R / 2) + q] = fma2(x.re, x.re, mul2(x.im, x.im));
+        }
+}
+
+// Output row of A-scan `row`. B-scan flip follows the reference CUDA kernel
+// (cuda_kernels.cu:553-573, launched at cuda_backend.cu:690-694): B-scan b is
+// mirrored laterally when b is even and b+1 < bscans, i.e. the first B-scan of
+// every complete pair; a trailing single B-scan is left as is.
+OPE_HD long long out_row(const ChainArgs& a, long long row) {
+    if (!a.flip) return row;
+    long long bs = row / a.ascans_per_bscan;
+    if ((bs & 1) != 0 || bs + 1 >= a.bscans) return row;
+    long long in_b = row - bs * a.ascans_per_bscan;
+    return bs * a.ascans_per_bscan + (a.ascans_per_bscan - 1 - in_b);
+}
+
+}  // namespace ope_b200

@@ -1,0 +1,139 @@
+// Host-side table builders (see tables.h). Compiled without FP contraction so
+// the float expressions round exactly as the reference's do.
+#include "tables.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+namespace ope_b200 {
+
+namespace {
+
+int trunc_index(float v) {
+    // static_cast<int>(float) truncates toward zero; non-finite or huge values
+    // (undefined in C++) are pinned so every table index stays in bounds.
+    if (!(v == v)) return 0;
+    if (v > 1.0e8f) return 100000000;
+    if (v < -1.0e8f) return -100000000;
+    return static_cast<int>(v);
+}
+
+int float_bits(float f) {
+    int b;
+    std::memcpy(&b, &f, 4);
+    return b;
+}
+
+}  // namespace
+
+float lanczos8(float x) {
+    if (std::fabs(x) < 1e-5f) return 1.0f;
+    if (std::fabs(x) >= 8.0f) return 0.0f;
+    const float pi = static_cast<float>(3.14159265358979323846);
+    const float px = pi * x;
+    const float pa = px / 8.0f;
+    return (sinf(px) / px) * (sinf(pa) / pa);
+}
+
+std::vector<float2> build_twiddles(int n) {
+    std::vector<float2> tw(n);
+    for (int j = 0; j < n; ++j) {
+        const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(j) / n;
+        tw[j] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
+    }
+    return tw;
+}
+
+std::vector<int2> build_linear_table(const float* curve, int n) {
+    std::vector<int2> tab(n);
+    for (int j = 0; j < n; ++j) {
+        const float nx = curve[j];
+        int n1 = trunc_index(nx);
+        if (n1 > n - 1) n1 = n - 1;
+        if (n1 < -SPEC_PAD) n1 = -SPEC_PAD;  // the reference would read out of bounds here
+        const float fr = nx - static_cast<float>(n1);
+        tab[j] = make_int2(n1 + SPEC_PAD, float_bits(fr));
+    }
+    return tab;
+}
+
+std::vector<int4> build_cubic_table(const float* curve, int n) {
+    std::vector<int4> tab(n);
+    auto cl = [n](int v) {
+        if (v > n - 1) v = n - 1;
+        if (v < -SPEC_PAD) v = -SPEC_PAD;
+        return v;
+    };
+    for (int j = 0; j < n; ++j) {
+        const float nx = curve[j];
+        const int i1 = trunc_index(nx);
+        const int n0 = cl(std::abs(i1 - 1)) + SPEC_PAD;
+        const int n1r = cl(i1);
+        const int n1 = n1r + SPEC_PAD;
+        const int n2 = cl(i1 + 1) + SPEC_PAD;
+        const int n3 = cl(i1 + 2) + SPEC_PAD;
+        const float pos = nx - static_cast<float>(n1r);
+        const float pos2 = pos * pos;
+        tab[j] = make_int4(n0 | (n1 << 16), n2 | (n3 << 16), float_bits(pos), float_bits(pos2));
+    }
+    return tab;
+}
+
+void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std::vector<float>& w) {
+    base.assign(n, 0);
+    w.assign(16 * static_cast<size_t>(n), 0.0f);
+    for (int j = 0; j < n; ++j) {
+        const float nx = curve[j];
+        const int n0 = trunc_index(nx);
+        for (int k = 0; k < 16; ++k) {
+            int idx = n0 - 7 + k;
+            if (idx < 0) idx = 0;
+            if (idx >= n) idx = n - 1;
+            w[static_cast<size_t>(k) * n + j] = lanczos8(nx - static_cast<float>(idx));
+        }
+        // Taps n0-7 .. n0+8 read the replicated edge padding when they leave
+        // [0, n); pinning n0 to [-9, n+7] keeps them inside it and reads the
+        // same clamped samples.
+        int b = n0;
+        if (b < -9) b = -9;
+        if (b > n + 7) b = n + 7;
+        base[j] = b - 7 + SPEC_PAD;
+    }
+}
+
+std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n) {
+    std::vector<float4> t(n);
+    for (int j = 0; j < n; ++j)
+        t[j] = make_float4(window ? window[j] : 1.0f, cos_sin ? cos_sin[2 * j] : 1.0f,
+                           cos_sin ? cos_sin[2 * j + 1] : 0.0f, 0.0f);
+    return t;
+}
+
+void scaling_constants(bool log_scaling, float gmin_f, float gmax_f, float addend_f, float mult_f, int n,
+                       ChainArgs& a) {
+    const double half = n / 2;
+    const double mult = mult_f, addend = addend_f, gmin = gmin_f;
+    // range in float as the reference computes it (cpu_kernels.tpp:332-335,356-361)
+    float rf = gmax_f - gmin_f;
+    if (rf < 1e-6f) rf = 1.0f;
+    const double range = rf;
+    a.mult = mult_f;
+    a.addend = addend_f;
+    if (log_scaling) {
+        // out = mult*((10 log10(|X|^2/(N/2)) - min)/range + addend)
+        const double c10 = 10.0 * std::log10(2.0);
+        a.log_mode = 1;
+        a.auto_minmax = (gmin_f == gmax_f) ? 1 : 0;
+        a.k_a = static_cast<float>(mult * c10 / range);
+        a.k_b = static_cast<float>(mult * ((-10.0 * std::log10(half) - gmin) / range + addend));
+    } else {
+        // out = mult*((|X|/(N/2) - min)/range + addend)
+        a.log_mode = 0;
+        a.auto_minmax = 0;
+        a.k_a = static_cast<float>(mult / (half * range));
+        a.k_b = static_cast<float>(mult * (addend - gmin / range));
+    }
+}
+
+}  // namespace ope_b200

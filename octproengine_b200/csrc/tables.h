@@ -1,0 +1,38 @@
+// Host-side builders of the device tables the chain kernels read. Pure C++
+// (no CUDA runtime calls) so the same code serves the C ABI and the CPU
+// emulation harness of the tests.
+#pragma once
+
+#include <vector>
+
+#include "chain_kernel.cuh"
+
+namespace ope_b200 {
+
+// lanczosKernel<float>(x, 8) of the reference (cpu_kernels.tpp:148-162),
+// evaluated with the same float operations.
+float lanczos8(float x);
+
+// W_N^j = exp(+2 pi i j / N), j < N, evaluated in double and rounded once.
+std::vector<float2> build_twiddles(int n);
+
+// kLinearizationLinear indices and fractions (cpu_kernels.tpp:95-110):
+// {n1 + SPEC_PAD, bits of float(nx - n1)}.
+std::vector<int2> build_linear_table(const float* curve, int n);
+
+// kLinearizationCubic indices (cpu_kernels.tpp:124-145), packed 16-bit and
+// offset by SPEC_PAD, plus pos and pos*pos as float bits.
+std::vector<int4> build_cubic_table(const float* curve, int n);
+
+// kLinearizationLanczos taps (cpu_kernels.tpp:176-195): per output index the
+// first gathered index (+ SPEC_PAD) and 16 weights (tap-major, 16 x n).
+void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std::vector<float>& w);
+
+// {window, cos, sin, 0}; a missing window is 1, a missing phase (cos 1, sin 0).
+std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n);
+
+// Output affine constants of logScaleAndTruncate / linearScaleAndTruncate
+// (cpu_kernels.tpp:301-378) folded for the kernel epilogue.
+void scaling_constants(bool log_scaling, float gmin, float gmax, float addend, float mult, int n, ChainArgs& a);
+
+}  // namespace ope_b200

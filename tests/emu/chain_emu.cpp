@@ -1,0 +1,225 @@
+// CPU emulation of the fused chain kernel. TEST INFRASTRUCTURE ONLY.
+//
+// Runs the kernel's own __host__ __device__ phase functions
+// (octproengine_b200/csrc/chain_kernel.cuh) for every thread of a team,
+// phase by phase, with the same shared-memory layout and with every shared
+// memory index bounds-checked (OPE_SMEM_CHECK asserts in the host build). It
+// lets the CPU test suite check the kernels' index arithmetic, the
+// bit-exactness of the pre-FFT stages and the FFT itself without a GPU. It is
+// never linked into the product.
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../octproengine_b200/csrc/chain_kernel.cuh"
+#include "../../octproengine_b200/csrc/tables.h"
+
+using namespace ope_b200;
+
+extern "C" {
+struct EmuArgs {
+    int n, in_kind, interp;
+    long long m;
+    const void* in;
+    const float* curve;
+    const float* window;
+    const float* cos_sin;
+    const float* fpn;  // interleaved n/2 pairs or null
+    int dc_window;
+    int log_scaling;
+    float gmin, gmax, addend, mult;
+    int flip, ascans_per_bscan, bscans;
+};
+}
+
+namespace {
+
+enum { OUT_IMAGE = 0, OUT_FFT_INPUT = 1, OUT_BINS = 2 };
+
+template <int N, int DT, int INTERP>
+int emu_run(const EmuArgs& e, int what, float* out) {
+    using PL = Plan<N>;
+    using LY = Layout<N, DT>;
+    using sum_t = typename InTraits<DT>::sum_t;
+    using raw_t = typename InTraits<DT>::raw_t;
+    constexpr int T = PL::T;
+    constexpr int NPASS = PL::NPASS;
+
+    std::vector<float2> tw = build_twiddles(N);
+    std::vector<int2> lin;
+    std::vector<int4> cub;
+    std::vector<int> lzb;
+    std::vector<float> lzw;
+    if (INTERP == INTERP_LINEAR) lin = build_linear_table(e.curve, N);
+    if (INTERP == INTERP_CUBIC) cub = build_cubic_table(e.curve, N);
+    if (INTERP == INTERP_LANCZOS) build_lanczos_table(e.curve, N, lzb, lzw);
+    std::vector<float4> wph = build_window_phase(e.window, e.cos_sin, N);
+
+    ChainArgs a{};
+    a.in = e.in;
+    a.m = e.m;
+    a.tw = tw.data();
+    a.lin = lin.data();
+    a.cub = cub.data();
+    a.lz_base = lzb.data();
+    a.lz_w = lzw.data();
+    a.wph = wph.data();
+    a.fpn = reinterpret_cast<const float2*>(e.fpn);
+    a.dc_window = e.dc_window;
+    scaling_constants(e.log_scaling != 0, e.gmin, e.gmax, e.addend, e.mult, N, a);
+    a.flip = e.flip;
+    a.ascans_per_bscan = e.ascans_per_bscan;
+    a.bscans = e.bscans;
+
+    std::vector<unsigned char> work(LY::WORK_BYTES + 64, 0);
+    std::vector<unsigned char> stage(LY::STAGE_BYTES, 0);
+    float2* spec = reinterpret_cast<float2*>(work.data() + LY::OFF_SPEC);
+    float4* exch = reinterpret_cast<float4*>(work.data() + LY::OFF_EXCH);
+    sum_t* pfx = reinterpret_cast<sum_t*>(work.data() + LY::OFF_PFX);
+    std::vector<std::array<cp, 16>> v(T);
+    const size_t row_bytes = N * sizeof(raw_t);
+    const unsigned char* in = static_cast<const unsigned char*>(e.in);
+
+    for (long long r = 0; r < e.m; r += 2) {
+        const bool has_b = r + 1 < e.m;
+        std::memcpy(stage.data(), in + r * row_bytes, row_bytes * (has_b ? 2 : 1));
+        if (!has_b) std::memset(stage.data() + row_bytes, 0, row_bytes);
+        if (e.dc_window > 0) {
+            std::vector<sum_t> ta(T), tb(T);
+            for (int t = 0; t < T; ++t) phase_dc_local<N, DT>(t, stage.data(), &ta[t], &tb[t]);
+            sum_t ea = 0, eb = 0;
+            for (int t = 0; t < T; ++t) {
+                sum_t xa = ta[t], xb = tb[t];
+                ta[t] = ea;
+                tb[t] = eb;
+                ea += xa;
+                eb += xb;
+            }
+            for (int t = 0; t < T; ++t) phase_dc_prefix<N, DT>(t, stage.data(), ta[t], tb[t], pfx);
+            for (int t = 0; t < T; ++t) phase_dc_apply<N, DT>(t, stage.data(), pfx, e.dc_window, spec);
+        } else {
+            for (int t = 0; t < T; ++t) phase_unpack<N, DT>(t, stage.data(), spec);
+        }
+        for (int t = 0; t < T; ++t) phase_prestage<N, INTERP>(t, spec, a, v[t].data());
+        if (what == OUT_FFT_INPUT) {
+            for (int t = 0; t < T; ++t)
+                for (int s = 0; s < 16; ++s) {
+                    const int j = t + s * T;
+                    const cp x = v[t][s];
+                    out[(r * N + j) * 2] = x.re.x;
+                    out[(r * N + j) * 2 + 1] = x.im.x;
+                    if (has_b) {
+                        out[((r + 1) * N + j) * 2] = x.re.y;
+                        out[((r + 1) * N + j) * 2 + 1] = x.im.y;
+                    }
+                }
+            continue;
+        }
+        for (int t = 0; t < T; ++t) fft_twiddle_dft<N, 0>(t, v[t].data(), tw.data());
+        for (int t = 0; t < T; ++t) fft_store<N, 0>(t, v[t].data(), exch);
+        if constexpr (NPASS > 2) {
+            for (int t = 0; t < T; ++t) {
+                fft_load<N>(t, exch, v[t].data());
+                fft_twiddle_dft<N, 1>(t, v[t].data(), tw.data());
+            }
+            for (int t = 0; t < T; ++t) fft_store<N, 1>(t, v[t].data(), exch);
+        }
+        if constexpr (NPASS > 3) {
+            for (int t = 0; t < T; ++t) {
+                fft_load<N>(t, exch, v[t].data());
+                fft_twiddle_dft<N, 2>(t, v[t].data(), tw.data());
+            }
+            for (int t = 0; t < T; ++t) fft_store<N, 2>(t, v[t].data(), exch);
+        }
+        for (int t = 0; t < T; ++t) {
+            fft_load<N>(t, exch, v[t].data());
+            fft_twiddle_dft<N, NPASS - 1>(t, v[t].data(), tw.data());
+        }
+        using L = LastInfo<N>;
+        if (what == OUT_BINS) {
+            for (int t = 0; t < T; ++t)
+                for (int i = 0; i < L::D; ++i)
+                    for (int q = 0; q < L::R / 2; ++q) {
+                        const int bin = L::bin(t, i, q);
+                        const cp x = v[t][i + q * L::D];
+                        out[(r * (N / 2) + bin) * 2] = x.re.x;
+                        out[(r * (N / 2) + bin) * 2 + 1] = x.im.x;
+                        if (has_b) {
+                            out[((r + 1) * (N / 2) + bin) * 2] = x.re.y;
+                            out[((r + 1) * (N / 2) + bin) * 2 + 1] = x.im.y;
+                        }
+                    }
+            continue;
+        }
+        // image epilogue (host restatement of the device epilogue; log2 is exact here)
+        std::vector<float> img(2 * (N / 2));
+        for (int t = 0; t < T; ++t) {
+            float2 mag2[L::NB];
+            epi_mag2<N>(t, v[t].data(), a, mag2);
+            for (int i = 0; i < L::D; ++i)
+                for (int q = 0; q < L::R / 2; ++q) {
+                    const int bin = L::bin(t, i, q);
+                    const float2 m2 = mag2[i * (L::R / 2) + q];
+                    img[bin] = a.log_mode ? std::log2(m2.x) : std::sqrt(m2.x);
+                    img[N / 2 + bin] = a.log_mode ? std::log2(m2.y) : std::sqrt(m2.y);
+                }
+        }
+        for (int lane = 0; lane < (has_b ? 2 : 1); ++lane) {
+            float* row = img.data() + lane * (N / 2);
+            if (a.log_mode && a.auto_minmax) {
+                const double c10 = 10.0 * std::log10(2.0);
+                float mn = INFINITY, mx = -INFINITY;
+                for (int b = 0; b < N / 2; ++b) {
+                    row[b] = static_cast<float>(c10 * row[b] - 10.0 * std::log10(N / 2.0));
+                    mn = std::fmin(mn, row[b]);
+                    mx = std::fmax(mx, row[b]);
+                }
+                float rg = mx - mn;
+                if (!(rg >= 1e-6f)) rg = 1.0f;
+                for (int b = 0; b < N / 2; ++b) row[b] = a.mult * ((row[b] - mn) / rg + a.addend);
+            } else {
+                for (int b = 0; b < N / 2; ++b) row[b] = std::fma(row[b], a.k_a, a.k_b);
+            }
+            const long long orow = out_row(a, r + lane);
+            std::memcpy(out + orow * (N / 2), row, sizeof(float) * (N / 2));
+        }
+    }
+    return 0;
+}
+
+template <int N, int DT>
+int by_interp(const EmuArgs& e, int what, float* out) {
+    switch (e.interp) {
+        case INTERP_NONE: return emu_run<N, DT, INTERP_NONE>(e, what, out);
+        case INTERP_LINEAR: return emu_run<N, DT, INTERP_LINEAR>(e, what, out);
+        case INTERP_CUBIC: return emu_run<N, DT, INTERP_CUBIC>(e, what, out);
+        case INTERP_LANCZOS: return emu_run<N, DT, INTERP_LANCZOS>(e, what, out);
+    }
+    return -1;
+}
+
+template <int N>
+int by_dt(const EmuArgs& e, int what, float* out) {
+    switch (e.in_kind) {
+        case IN_U8: return by_interp<N, IN_U8>(e, what, out);
+        case IN_U16: return by_interp<N, IN_U16>(e, what, out);
+        case IN_U32: return by_interp<N, IN_U32>(e, what, out);
+        case IN_F32: return by_interp<N, IN_F32>(e, what, out);
+    }
+    return -1;
+}
+
+}  // namespace
+
+extern "C" int emu_chain(const EmuArgs* e, int what, float* out) {
+    switch (e->n) {
+        case 512: return by_dt<512>(*e, what, out);
+        case 1024: return by_dt<1024>(*e, what, out);
+        case 2048: return by_dt<2048>(*e, what, out);
+        case 4096: return by_dt<4096>(*e, what, out);
+        case 8192: return by_dt<8192>(*e, what, out);
+    }
+    return -1;
+}

@@ -1,0 +1,172 @@
+"""The chain kernel's own phase functions, run on the CPU by tests/emu, against
+the oracle: the pre-FFT stages bit for bit, the FFT to float32 accuracy, the
+output within the stated tolerances. Every shared-memory index is
+bounds-checked by the emulation."""
+import numpy as np
+import pytest
+
+import helpers as H
+from octproengine_b200.chain import ChainSpec, UINT8, UINT16, UINT32, FLOAT32, LINEAR, CUBIC, LANCZOS
+from oracle import restate as R
+
+NS = [512, 1024, 2048, 4096, 8192]
+INTERPS = [None, LINEAR, CUBIC, LANCZOS]
+
+
+def spec_for(n, interp, dtype=UINT16, m=5, **kw):
+    base = dict(signal_length=n, ascans_per_bscan=m, input_dtype=dtype, resampling=interp is not None,
+                interpolation=interp or 0, resampling_coeffs=(0.5, n, -100.0, 50.0), windowing=True,
+                window_type=0, window_center=0.5, window_fill=0.9, dispersion=True,
+                dispersion_coeffs=(0.0, 0.0, 1.0, -3.0), grayscale_min=0.0, grayscale_max=80.0)
+    base.update(kw)
+    return ChainSpec(**base)
+
+
+@pytest.mark.parametrize("interp", INTERPS)
+@pytest.mark.parametrize("n", NS)
+def test_fft_input_bit_exact(emu, n, interp):
+    spec = spec_for(n, interp)
+    raw = H.random_raw(spec, seed=n)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    st, cur = H.oracle_settings(spec)
+    assert np.array_equal(z.astype(np.complex64), R.fft_input(raw, st, cur))
+
+
+@pytest.mark.parametrize("dtype", [UINT8, UINT16, UINT32, FLOAT32])
+def test_fft_input_dtypes_bit_exact(emu, dtype):
+    spec = spec_for(1024, CUBIC, dtype=dtype, m=3)
+    raw = H.random_raw(spec, seed=dtype)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    st, cur = H.oracle_settings(spec)
+    assert np.array_equal(z.astype(np.complex64), R.fft_input(raw, st, cur))
+
+
+def test_float32_as_uint32_quirk(emu):
+    """With float32_as_uint32 the bytes are read as uint32 (cpu_kernels.tpp:47-52)."""
+    spec = spec_for(512, LINEAR, dtype=FLOAT32, m=2, float32_as_uint32=True)
+    raw = H.random_raw(spec, seed=3)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    st, cur = H.oracle_settings(spec)
+    assert np.array_equal(z.astype(np.complex64), R.fft_input(raw, st, cur))
+
+
+@pytest.mark.parametrize("n", NS)
+def test_fft_accuracy(emu, n):
+    spec = spec_for(n, LINEAR, m=4)
+    raw = H.random_raw(spec, seed=1)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    X = H.emu_run(emu, spec, raw, "bins")
+    X64 = R.inverse_dft(z)[:, : n // 2]
+    rel = np.abs(X - X64).max() / np.abs(X64).max()
+    assert rel < 4e-7, rel
+
+
+@pytest.mark.parametrize("n", [512, 2048, 8192])
+def test_dc_removal_exact_rolling_mean(emu, n):
+    """Rolling-average DC removal uses exact integer window sums: the spectrum
+    matches the float64 evaluation of the reference formula to float32
+    rounding (the reference's own float prefix sum is less accurate)."""
+    spec = spec_for(n, CUBIC, m=4, dc_removal=True, dc_window=64)
+    raw = H.random_raw(spec, seed=2)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    st, cur = H.oracle_settings(spec)
+    z64 = R.fft_input(raw, st, cur, mode="f64")
+    zref = R.fft_input(raw, st, cur)
+    err_gpu = np.abs(z - z64).max()
+    err_ref = np.abs(zref - z64).max()
+    assert err_gpu < 4e-3
+    assert err_gpu <= err_ref
+
+
+def test_dc_removal_small_sums_bit_exact(emu):
+    """While the reference's float prefix sum stays below 2^24 it is exact and
+    both agree bit for bit (uint8 input)."""
+    spec = spec_for(1024, LINEAR, dtype=UINT8, m=4, dc_removal=True, dc_window=32)
+    raw = H.random_raw(spec, seed=9)
+    z = H.emu_run(emu, spec, raw, "fft_input")
+    st, cur = H.oracle_settings(spec)
+    assert np.array_equal(z.astype(np.complex64), R.fft_input(raw, st, cur))
+
+
+@pytest.mark.parametrize("n", [512, 2048, 4096])
+@pytest.mark.parametrize("interp", INTERPS)
+def test_image_vs_oracle(emu, n, interp):
+    spec = spec_for(n, interp, m=6)
+    raw = H.random_raw(spec, seed=5)
+    img = H.emu_run(emu, spec, raw, "image")
+    ref = H.oracle_image(spec, raw).output
+    db = np.abs(H.to_db(img, spec) - H.to_db(ref, spec))
+    assert db.max() < 5e-3, db.max()
+
+
+def test_odd_count_single_row_last_pair(emu):
+    spec = spec_for(1024, LINEAR, m=7)
+    raw = H.random_raw(spec, seed=4)
+    img = H.emu_run(emu, spec, raw, "image")
+    ref = H.oracle_image(spec, raw).output
+    assert np.abs(H.to_db(img, spec) - H.to_db(ref, spec)).max() < 5e-3
+
+
+def test_linear_scaling(emu):
+    spec = spec_for(1024, CUBIC, m=4, log_scaling=False, grayscale_min=0.0, grayscale_max=3.0, multiplicator=2.0,
+                    addend=0.25)
+    raw = H.random_raw(spec, seed=6)
+    img = H.emu_run(emu, spec, raw, "image")
+    ref = H.oracle_image(spec, raw).output
+    # FFT rounding is relative to the strongest bin of the A-scan
+    assert np.abs(img - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+def test_auto_minmax(emu):
+    spec = spec_for(2048, None, m=4, grayscale_min=40.0, grayscale_max=40.0, multiplicator=1.5, addend=0.1)
+    raw = H.random_raw(spec, seed=8)
+    img = H.emu_run(emu, spec, raw, "image")
+    ref = H.oracle_image(spec, raw).output
+    np.testing.assert_allclose(img, ref, rtol=0, atol=2e-5)
+
+
+def test_fpn_profile_subtraction(emu):
+    spec = spec_for(1024, LINEAR, m=4, fpn_removal=True)
+    raw = H.random_raw(spec, seed=10)
+    rng = np.random.default_rng(1)
+    prof = (rng.normal(0, 2000, 1024)).astype(np.float32)  # 512 complex pairs
+    img = H.emu_run(emu, spec, raw, "image", fpn=prof)
+    ref = H.oracle_image(spec, raw, fpn_profile=prof).output
+    assert np.abs(H.to_db(img, spec) - H.to_db(ref, spec)).max() < 5e-3
+
+
+def test_bscan_flip_row_mapping(emu):
+    """Flip mirrors B-scan b laterally when b is even and b+1 exists
+    (cuda_kernels.cu:553-573): B-scans 0 and 2 of 3 -> only 0 is flipped."""
+    base = spec_for(512, LINEAR, m=4, ascans_per_bscan=4, bscans_per_buffer=3)
+    raw = H.random_raw(base, seed=11)
+    a = H.emu_run(emu, base, raw, "image")
+    b = H.emu_run(emu, base.with_(bscan_flip=True), raw, "image")
+    assert np.array_equal(b[0:4], a[0:4][::-1])
+    assert np.array_equal(b[4:12], a[4:12])
+
+
+@pytest.mark.parametrize("case", H.golden_cases(), ids=lambda c: c[0])
+def test_emulated_kernel_vs_golden(emu, case):
+    """Kernel error against float64 is no larger than the reference's own error
+    when its DFT runs in float32 (``out_f32fft``), and small on the display
+    range [grayscale_min, inf) in dB."""
+    name, spec, d = case
+    fpn = d["fpn"] if spec.fpn_removal else None
+    img = H.emu_run(emu, spec, d["raw"], "image", fpn=fpn)
+    st, cur = H.oracle_settings(spec)
+    f64 = R.process_buffer(d["raw"], st, cur, mode="f64", fpn_profile=fpn).output
+    ref32 = d["out_f32fft"]
+    if spec.log_scaling and spec.grayscale_min != spec.grayscale_max:
+        k_db, r_db, t_db = H.to_db(img, spec), H.to_db(ref32, spec), H.to_db(f64, spec)
+        err_kernel = np.abs(k_db - t_db)
+        err_ref = np.abs(r_db - t_db)
+        assert err_kernel.max() <= max(2.0 * err_ref.max(), 5e-3)
+        display = t_db >= spec.grayscale_min
+        assert err_kernel[display].max() < 1e-2
+    else:
+        # linear scaling, or log scaling with the automatic per-A-scan range
+        # (normalised by the weakest bin, whose float32 error is largest)
+        err_kernel = np.abs(img.astype(np.float64) - f64).max()
+        err_ref = np.abs(ref32.astype(np.float64) - f64).max()
+        assert err_kernel <= max(2.0 * err_ref, 1e-5 * np.abs(f64).max())

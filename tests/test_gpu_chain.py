@@ -1,0 +1,213 @@
+"""GPU parity of the fused chain, called through the C ABI (include/ope_b200.h).
+
+* complex bins: bit-identical to the CPU emulation of the same kernel code
+  (whose pre-FFT stages are bit-identical to the oracle restatement, itself
+  pinned to the reference);
+* images: against the oracle and the golden fixtures with the tolerances of
+  tests/test_emulator.py;
+* full-size buffers: size-independent properties (A-scan permutation and
+  buffer splitting leave every output bit unchanged; repeated runs are
+  identical);
+* error paths: misaligned buffers and a bounded wait that runs out.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+from octproengine_b200 import capi
+from octproengine_b200.chain import (ChainSpec, open_context, UINT8, UINT16, UINT32, FLOAT32, LINEAR, CUBIC,
+                                     LANCZOS, GAUSS, HANN)
+from oracle import restate as R
+
+pytestmark = pytest.mark.gpu
+
+NS = [512, 1024, 2048, 4096, 8192]
+INTERPS = [None, LINEAR, CUBIC, LANCZOS]
+
+
+def spec_for(n, interp, dtype=UINT16, m=5, **kw):
+    base = dict(signal_length=n, ascans_per_bscan=m, input_dtype=dtype, resampling=interp is not None,
+                interpolation=interp or 0, resampling_coeffs=(0.5, n, -100.0, 50.0), windowing=True,
+                window_type=HANN, window_center=0.5, window_fill=0.9, dispersion=True,
+                dispersion_coeffs=(0.0, 0.0, 1.0, -3.0), grayscale_min=0.0, grayscale_max=80.0)
+    base.update(kw)
+    return ChainSpec(**base)
+
+
+@pytest.mark.parametrize("interp", INTERPS)
+@pytest.mark.parametrize("n", NS)
+def test_bins_bit_identical_to_emulation(cuda, emu, n, interp):
+    spec = spec_for(n, interp, m=7)
+    raw = H.random_raw(spec, seed=n + 1)
+    g = H.gpu_run(spec, raw, "bins")
+    e = H.emu_run(emu, spec, raw, "bins")
+    assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
+
+
+@pytest.mark.parametrize("dtype", [UINT8, UINT16, UINT32, FLOAT32])
+@pytest.mark.parametrize("dc", [False, True])
+def test_dtypes_and_dc_bit_identical_to_emulation(cuda, emu, dtype, dc):
+    spec = spec_for(2048, CUBIC, dtype=dtype, m=6, dc_removal=dc, dc_window=64)
+    raw = H.random_raw(spec, seed=dtype)
+    g = H.gpu_run(spec, raw, "bins")
+    e = H.emu_run(emu, spec, raw, "bins")
+    assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
+
+
+@pytest.mark.parametrize("interp", INTERPS)
+@pytest.mark.parametrize("n", [512, 2048, 8192])
+def test_image_vs_oracle(cuda, n, interp):
+    spec = spec_for(n, interp, m=9)
+    raw = H.random_raw(spec, seed=3)
+    img = H.gpu_run(spec, raw)
+    ref = H.oracle_image(spec, raw).output
+    f64 = H.oracle_image(spec, raw, mode="f64").output
+    err_gpu = np.abs(H.to_db(img, spec) - H.to_db(f64, spec)).max()
+    err_cpu = np.abs(H.to_db(ref, spec) - H.to_db(f64, spec)).max()
+    assert np.abs(H.to_db(img, spec) - H.to_db(ref, spec)).max() < 1e-2
+    assert err_gpu < 1e-2, (err_gpu, err_cpu)
+
+
+@pytest.mark.parametrize("case", H.golden_cases(), ids=lambda c: c[0])
+def test_golden_fixtures(cuda, case):
+    name, spec, d = case
+    fpn = d["fpn"] if spec.fpn_removal else None
+    img = H.gpu_run(spec, d["raw"], fpn_profile=fpn)
+    st, cur = H.oracle_settings(spec)
+    f64 = R.process_buffer(d["raw"], st, cur, mode="f64", fpn_profile=fpn).output
+    ref32 = d["out_f32fft"]
+    if spec.log_scaling and spec.grayscale_min != spec.grayscale_max:
+        k_db, r_db, t_db = H.to_db(img, spec), H.to_db(ref32, spec), H.to_db(f64, spec)
+        err_kernel = np.abs(k_db - t_db)
+        assert err_kernel.max() <= max(2.0 * np.abs(r_db - t_db).max(), 5e-3)
+        assert err_kernel[t_db >= spec.grayscale_min].max() < 1e-2
+    else:
+        err_kernel = np.abs(img.astype(np.float64) - f64).max()
+        err_ref = np.abs(ref32.astype(np.float64) - f64).max()
+        assert err_kernel <= max(2.0 * err_ref, 1e-5 * np.abs(f64).max())
+
+
+def test_fpn_determination_matches_oracle(cuda):
+    """requestFixedPatternNoiseDetermination + removal in one frame, as
+    computeFixedPatternNoiseIfRequested (cpu_backend.cpp:305-357) does for the
+    first frame: profile from the first fpn_bscan_count*A A-scans."""
+    spec = spec_for(1024, CUBIC, m=64, ascans_per_bscan=64, bscans_per_buffer=2, fpn_removal=True,
+                    grayscale_min=20.0, grayscale_max=110.0)
+    raw = H.random_raw(spec, seed=21)
+    ctx = open_context(spec)
+    try:
+        img = H.gpu_run(spec, raw, ctx=ctx, fpn_request=True)
+        prof = ctx.fpn_profile()
+    finally:
+        ctx.close()
+    res = H.oracle_image(spec, raw, determine_fpn=True)
+    assert prof.size == spec.signal_length  # N/2 complex pairs
+    scale = np.abs(res.fpn_profile).max()
+    assert np.abs(prof - res.fpn_profile).max() <= 1e-5 * scale
+    f64 = H.oracle_image(spec, raw, mode="f64", fpn_profile=res.fpn_profile).output
+    err = np.abs(H.to_db(img, spec) - H.to_db(f64, spec))
+    assert err[H.to_db(f64, spec) >= spec.grayscale_min].max() < 1e-2
+
+
+def test_fpn_accumulates_across_buffers(cuda):
+    """fpn_bscan_count larger than one buffer: the determination completes on
+    the buffer that brings the count to fpn_bscan_count*A A-scans."""
+    spec = spec_for(512, LINEAR, m=32, ascans_per_bscan=32, bscans_per_buffer=1, fpn_removal=True,
+                    fpn_bscan_count=2)
+    r1 = H.random_raw(spec, seed=31)
+    r2 = H.random_raw(spec, seed=32)
+    ctx = open_context(spec)
+    try:
+        ctx.request_fpn_determination()
+        H.gpu_run(spec, r1, ctx=ctx)
+        assert ctx.fpn_profile().size == 0
+        H.gpu_run(spec, r2, ctx=ctx)
+        prof = ctx.fpn_profile()
+    finally:
+        ctx.close()
+    st, cur = H.oracle_settings(spec)
+    X = R.inverse_dft(R.fft_input(np.concatenate([r1, r2]), st, cur)).astype(np.complex64)
+    want = R.min_var_mean(X, 8)[:512]
+    assert np.abs(prof - want).max() <= 1e-5 * np.abs(want).max()
+
+
+def test_full_size_properties(cuda):
+    """2048 x 1024 x 8 uint16: A-scans are independent, so permuting the input
+    rows permutes the output rows and splitting the buffer changes nothing,
+    bit for bit; a sample of rows matches the oracle."""
+    import torch
+    spec = spec_for(2048, LANCZOS, m=1024, ascans_per_bscan=1024, bscans_per_buffer=8, window_type=GAUSS)
+    m = spec.num_ascans
+    from octproengine_b200 import synth
+    x = synth.generate(synth.SynthParams(n=2048, ascans=1024, bscans=8, seed=5), device="cuda:0")
+    ctx = open_context(spec)
+    try:
+        out = torch.empty((m, 1024), dtype=torch.float32, device="cuda:0")
+        s = torch.cuda.current_stream().cuda_stream
+        ctx.process_device(x.data_ptr(), out.data_ptr(), s)
+        out2 = torch.empty_like(out)
+        ctx.process_device(x.data_ptr(), out2.data_ptr(), s)
+        perm = torch.randperm(m, generator=torch.Generator().manual_seed(0)).to("cuda:0")
+        xp = x[perm].contiguous()
+        outp = torch.empty_like(out)
+        ctx.process_device(xp.data_ptr(), outp.data_ptr(), s)
+        half = m // 2 + 1
+        outs = torch.empty_like(out)
+        ctx.process_device(x.data_ptr(), outs.data_ptr(), s, num_ascans=half)
+        ctx.process_device(x[half:].contiguous().data_ptr(), outs[half:].data_ptr(), s, num_ascans=m - half)
+        torch.cuda.synchronize()
+        assert ctx.synchronize() == 0
+    finally:
+        ctx.close()
+    assert torch.equal(out, out2)
+    assert torch.equal(outp, out[perm])
+    assert torch.equal(outs, out)
+    rows = np.array([0, 1, 777, 4096, m - 1])
+    raw = x[torch.from_numpy(rows).to("cuda:0")].cpu().numpy().view(np.uint16)
+    ref = H.oracle_image(spec.with_(ascans_per_bscan=len(rows), bscans_per_buffer=1), raw).output
+    got = out[torch.from_numpy(rows).to("cuda:0")].cpu().numpy()
+    assert np.abs(H.to_db(got, spec) - H.to_db(ref, spec)).max() < 1e-2
+
+
+def test_misaligned_input_rejected(cuda):
+    import torch
+    spec = spec_for(512, LINEAR, m=4)
+    ctx = open_context(spec)
+    try:
+        buf = torch.zeros(512 * 4 * 2 + 64, dtype=torch.uint8, device="cuda:0")
+        out = torch.empty((4, 256), dtype=torch.float32, device="cuda:0")
+        with pytest.raises(capi.B200Error) as ei:
+            ctx.process_device(buf.data_ptr() + 2, out.data_ptr())
+        assert ei.value.code == capi.E_INVALID
+    finally:
+        ctx.close()
+
+
+def test_bounded_wait_reports_timeout_and_context_recovers(cuda):
+    """The first input copy is withheld: the kernel's bounded wait runs out,
+    it records a status and returns; the next frame on the same context is
+    correct."""
+    spec = spec_for(1024, LINEAR, m=6)
+    raw = H.random_raw(spec, seed=2)
+    ctx = open_context(spec)
+    try:
+        ctx.inject_copy_stall(2000)  # 2 ms
+        with pytest.raises(AssertionError):
+            H.gpu_run(spec, raw, ctx=ctx)  # synchronize() reports the status
+        img = H.gpu_run(spec, raw, ctx=ctx)
+    finally:
+        ctx.close()
+    ref = H.oracle_image(spec, raw).output
+    assert np.abs(H.to_db(img, spec) - H.to_db(ref, spec)).max() < 1e-2
+
+
+def test_process_host_roundtrip(cuda):
+    spec = spec_for(2048, CUBIC, m=12)
+    raw = H.random_raw(spec, seed=4)
+    ctx = open_context(spec)
+    try:
+        a = ctx.process_host(raw)
+    finally:
+        ctx.close()
+    b = H.gpu_run(spec, raw)
+    assert np.array_equal(a, b)
