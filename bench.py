@@ -212,7 +212,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    spec = bench_spec().with_(device=local)
+    from octproengine_b200.chain import LINEAR, CUBIC
+    interp = {"linear": LINEAR, "cubic": CUBIC, "lanczos": LANCZOS}[args.interp]
+    spec = bench_spec(interp).with_(device=local, bscans_per_buffer=BSCANS)
     M = spec.num_ascans
     x = synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=BSCANS, seed=100 + rank,
                                          background_ripple=True), device=dev)
@@ -258,8 +260,18 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     tpa = profile_traffic_per_ascan()
 
-    # Lanczos variant and FPN determination frame (same buffer)
     variants = {}
+    if args.kernel_only:
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_step,
+                              "kernel_only": True, "bscans": BSCANS, "interp": args.interp,
+                              "hbm_frac": (M * algorithmic_bytes_per_ascan() / (ms / args.steps / 1e3) / 1e9)
+                              / measured_peak()[0]}), flush=True)
+        return 0
+    # Lanczos variant and FPN determination frame (same buffer)
     spec_l = spec.with_(interpolation=LANCZOS)
     ctx_l = open_context(spec_l)
     ctx_l.set_fpn_profile(ctx.fpn_profile())
@@ -342,15 +354,21 @@ def run_ours(args):
 
 
 def main():
+    global BSCANS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bscans", type=int, default=BSCANS, help="B-scans per buffer (profiling uses fewer)")
+    ap.add_argument("--interp", default="cubic", choices=["linear", "cubic", "lanczos"])
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only the timed device loop (for ncu captures): no variants, e2e or CPU baseline")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    BSCANS = args.bscans
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -85,7 +85,11 @@ typedef struct ope_b200_config {
                                   backends do (cpu_kernels.tpp:47-52); 0: as float */
     int32_t device;            /* CUDA device ordinal                           */
     int32_t num_input_buffers; /* host input ring depth (>= 2)                  */
-    int32_t reserved[9];
+    int32_t dc_split;          /* 1 (default): exact DC split -- each A-scan's integer
+                                  mean is subtracted before the chain and its float64
+                                  response added back after the DFT (same quantity,
+                                  lower float32 error; ignored with DC removal on) */
+    int32_t reserved[8];
 } ope_b200_config;
 
 typedef struct ope_b200_ctx ope_b200_ctx;

@@ -71,7 +71,8 @@ class Config(ctypes.Structure):
         ("float32_as_uint32", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("num_input_buffers", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 9),
+        ("dc_split", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 8),
     ]
 
 

@@ -53,6 +53,7 @@ class ChainSpec:
     fpn_continuous: bool = False
     bscan_flip: bool = False
     float32_as_uint32: bool = False
+    dc_split: bool = True
     device: int = 0
     # custom curves (used instead of the generated ones when given)
     resampling_curve: Optional[np.ndarray] = field(default=None, repr=False)
@@ -92,6 +93,7 @@ class ChainSpec:
         c.fpn_continuous = int(self.fpn_continuous)
         c.bscan_flip = int(self.bscan_flip)
         c.float32_as_uint32 = int(self.float32_as_uint32)
+        c.dc_split = int(self.dc_split)
         c.device = int(self.device)
         return c
 

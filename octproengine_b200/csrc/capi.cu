@@ -63,6 +63,8 @@ struct TableSlot {
     int* lzb = nullptr;
     float* lzw = nullptr;
     float4* wph = nullptr;
+    float2* dcr = nullptr;  // DC response for the exact DC split (n/2)
+    bool has_dcr = false;
     cudaEvent_t last_use = nullptr;
 };
 
@@ -158,6 +160,7 @@ void free_slot(TableSlot& s) {
     cudaFree(s.lzb);
     cudaFree(s.lzw);
     cudaFree(s.wph);
+    cudaFree(s.dcr);
     if (s.last_use) cudaEventDestroy(s.last_use);
     s = TableSlot{};
 }
@@ -172,6 +175,7 @@ int rebuild_tables(ope_b200_ctx* c) {
 
     // resampling
     c->interp = INTERP_NONE;
+    std::vector<float> lz_w;
     if (cfg.resampling_enabled) {
         if (c->resample.size() != static_cast<size_t>(n))
             return fail(c, OPE_B200_E_STATE, "resampling enabled but no curve of length N was set");
@@ -186,8 +190,8 @@ int rebuild_tables(ope_b200_ctx* c) {
             c->interp = INTERP_CUBIC;
         } else {
             std::vector<int> base;
-            std::vector<float> w;
-            build_lanczos_table(c->resample.data(), n, base, w);
+            build_lanczos_table(c->resample.data(), n, base, lz_w);
+            std::vector<float>& w = lz_w;
             OPE_CU(c, cudaMemcpy(s.lzb, base.data(), n * sizeof(int), cudaMemcpyHostToDevice));
             OPE_CU(c, cudaMemcpy(s.lzw, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
             c->interp = INTERP_LANCZOS;
@@ -202,6 +206,14 @@ int rebuild_tables(ope_b200_ctx* c) {
     const bool disp = cfg.dispersion_enabled && c->cos_sin.size() == 2 * static_cast<size_t>(n);
     std::vector<float4> wph = build_window_phase(win ? c->window.data() : nullptr, disp ? c->cos_sin.data() : nullptr, n);
     OPE_CU(c, cudaMemcpy(s.wph, wph.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    // exact DC split: not needed when the rolling-average DC removal is on
+    s.has_dcr = cfg.dc_split && !cfg.dc_removal_enabled;
+    if (s.has_dcr) {
+        std::vector<float2> d = build_dc_response(n, c->interp, lz_w.empty() ? nullptr : lz_w.data(),
+                                                  win ? c->window.data() : nullptr,
+                                                  disp ? c->cos_sin.data() : nullptr);
+        OPE_CU(c, cudaMemcpy(s.dcr, d.data(), (n / 2) * sizeof(float2), cudaMemcpyHostToDevice));
+    }
     c->active = target;
     c->tables_dirty = false;
     return OPE_B200_OK;
@@ -214,6 +226,7 @@ int alloc_slot(ope_b200_ctx* c, TableSlot& s) {
     OPE_CU(c, cudaMalloc(&s.lzb, n * sizeof(int)));
     OPE_CU(c, cudaMalloc(&s.lzw, 16 * n * sizeof(float)));
     OPE_CU(c, cudaMalloc(&s.wph, n * sizeof(float4)));
+    OPE_CU(c, cudaMalloc(&s.dcr, (n / 2) * sizeof(float2)));
     OPE_CU(c, cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
     return OPE_B200_OK;
 }
@@ -246,6 +259,8 @@ static ChainArgs make_args(ope_b200_ctx* c, const void* d_in, float* d_out, long
     a.bscans = static_cast<int>((m + c->cfg.ascans_per_bscan - 1) / c->cfg.ascans_per_bscan);
     a.status = c->d_status;
     a.timeout_ns = 2000000000ull;
+    a.neg_zero = -0.0f;
+    a.dc_resp = s.has_dcr ? s.dcr : nullptr;
     return a;
 }
 
@@ -277,6 +292,7 @@ void ope_b200_config_default(ope_b200_config* c) {
     c->bg_weight = 1.0f;
     c->bg_offset = 0.0f;
     c->num_input_buffers = 2;
+    c->dc_split = 1;
 }
 
 int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out) {

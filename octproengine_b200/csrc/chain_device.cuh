@@ -94,6 +94,30 @@ __device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
     b = pb + ib - b;
 }
 
+// Team sum of two doubles, in a fixed order (xor butterfly inside each warp,
+// then warp totals in warp order) that the CPU emulation reproduces.
+template <int T>
+__device__ __forceinline__ void team_sum2(double& a, double& b, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+        scratch[2 * warp] = a;
+        scratch[2 * warp + 1] = b;
+    }
+    __syncthreads();
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < T / 32; ++w) {
+        ta += scratch[2 * w];
+        tb += scratch[2 * w + 1];
+    }
+    a = ta;
+    b = tb;
+}
+
 template <int T>
 __device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scratch) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -123,11 +147,12 @@ __device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scra
 
 // Output stage for one pair: scaling, affine map, streaming stores.
 template <int N>
-__device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a, long long row_a, float* scratch) {
+__device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a, long long row_a, float2 dc,
+                                         float* scratch) {
     using L = LastInfo<N>;
     constexpr int NB = L::NB;
     float2 mag2[NB];
-    epi_mag2<N>(t, v, a, mag2);
+    epi_mag2<N>(t, v, a, dc, mag2);
     float2 res[NB];
     if (a.log_mode) {
 #pragma unroll
@@ -238,7 +263,8 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
         }
         const unsigned char* stage = stages + st * LY::STAGE_BYTES;
 
-        // ---- unpack (+ DC removal) ----
+        // ---- unpack (+ DC removal or exact DC split) ----
+        float2 dc = make_float2(0.0f, 0.0f);
         if (a.dc_window > 0) {
             sum_t ta, tb;
             phase_dc_local<N, DT>(t, stage, &ta, &tb);
@@ -246,6 +272,13 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
             phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
             __syncthreads();
             phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
+        } else if (a.dc_resp) {
+            float2 vals[16];
+            double sa, sb;
+            phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
+            team_sum2<T>(sa, sb, reinterpret_cast<double*>(scan));
+            dc = make_float2(split_level(sa, N, DT != IN_F32), split_level(sb, N, DT != IN_F32));
+            phase_split_store<N>(t, vals, dc, spec);
         } else {
             phase_unpack<N, DT>(t, stage, spec);
         }
@@ -275,7 +308,7 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
         fft_load<N>(t, exch, v);
         fft_twiddle_dft<N, NPASS - 1>(t, v, a.tw);
         const long long ra = row0 + 2 * item;
-        sink(t, v, ra, ra + 1 < row_end);
+        sink(t, v, ra, ra + 1 < row_end, dc);
         __syncthreads();  // next item overwrites spec/exch
     }
 }
@@ -284,7 +317,7 @@ template <int N>
 struct ImageSink {
     const ChainArgs& a;
     float* scratch;
-    __device__ __forceinline__ void operator()(int t, const cp* v, long long row_a, bool has_b) {
+    __device__ __forceinline__ void operator()(int t, const cp* v, long long row_a, bool has_b, float2 dc) {
         if (a.bins_out) {
             // complex bins after the (optional) FPN subtraction, before magnitude
             using L = LastInfo<N>;
@@ -293,7 +326,7 @@ struct ImageSink {
 #pragma unroll
                 for (int q = 0; q < L::R / 2; ++q) {
                     const int bin = L::bin(t, i, q);
-                    cp x = v[i + q * L::D];
+                    cp x = add_dc(a, v[i + q * L::D], bin, dc);
                     if (a.fpn) {
                         const float2 f = __ldg(a.fpn + bin);
                         x.re = sub2(x.re, dup2(f.x));
@@ -304,7 +337,7 @@ struct ImageSink {
                 }
             return;
         }
-        epilogue<N>(t, v, a, row_a, scratch);
+        epilogue<N>(t, v, a, row_a, dc, scratch);
     }
 };
 
@@ -328,17 +361,17 @@ template <int N>
 struct FpnStatsSink {
     using L = LastInfo<N>;
     double acc[L::NB][3];
-    const float2* fpn_unused;
     __device__ __forceinline__ void reset() {
 #pragma unroll
         for (int k = 0; k < L::NB; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
     }
-    __device__ __forceinline__ void operator()(int, const cp* v, long long, bool has_b) {
+    const ChainArgs* args;
+    __device__ __forceinline__ void operator()(int t, const cp* v, long long, bool has_b, float2 dc) {
 #pragma unroll
         for (int i = 0; i < L::D; ++i)
 #pragma unroll
             for (int q = 0; q < L::R / 2; ++q) {
-                const cp x = v[i + q * L::D];
+                const cp x = add_dc(*args, v[i + q * L::D], L::bin(t, i, q), dc);
                 const int k = i * (L::R / 2) + q;
                 double re = x.re.x, im = x.im.x;
                 acc[k][0] += re;
@@ -368,6 +401,7 @@ __global__ void __launch_bounds__(N / 16) fpn_stats_kernel(const ChainArgs a, lo
     long long lo = (glo > g0 ? glo : g0) - g0;
     long long hi = (ghi < g0 + rows ? ghi : g0 + rows) - g0;
     FpnStatsSink<N> sink;
+    sink.args = &a;
     sink.reset();
     if (hi > lo) {
         const long long npairs = (hi - lo + 1) / 2;

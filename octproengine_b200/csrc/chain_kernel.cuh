@@ -71,6 +71,13 @@ struct ChainArgs {
     unsigned long long timeout_ns;
     float2* bins_out;    // if set: write complex bins [0, N/2) per A-scan instead of the image
     int debug_skip_first_copy;  // test hook: never issue the first bulk copy (exercises the timeout path)
+    float neg_zero;      // -0.0f, passed at run time (see mul2x in pair_math.cuh)
+    // Exact DC split: when set, each A-scan's integer mean c is subtracted
+    // exactly before the chain and c * dc_resp[k] added back after the DFT.
+    // dc_resp[k] (k < N/2) is the chain's response to a constant 1 spectrum,
+    // evaluated in float64; the chain is linear up to the DFT, so the result
+    // is the same quantity computed with a far smaller float32 error floor.
+    const float2* dc_resp;
 };
 
 template <int N_>
@@ -227,6 +234,56 @@ OPE_HD void phase_unpack(int t, const unsigned char* stage, float2* spec) {
     }
 }
 
+// Exact DC split, step A: thread t loads its two 8-sample chunks (kept in
+// registers across the team reduction) and sums each row in double.
+template <int N, int DT>
+OPE_HD void phase_split_load(int t, const unsigned char* stage, float2* vals, double* sa, double* sb) {
+    constexpr int T = Plan<N>::T;
+    double a = 0.0, b = 0.0;
+    int idx = 0;
+#pragma unroll
+    for (int c = t; c < N / 8; c += T, ++idx) {
+        load_chunk8<DT>(stage, N, c, vals + 8 * idx);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a += (double)vals[8 * idx + k].x;
+            b += (double)vals[8 * idx + k].y;
+        }
+    }
+    *sa = a;
+    *sb = b;
+}
+
+// The subtracted level of one A-scan: its mean rounded to an integer for
+// integer samples (so x - c is exact in float), the plain mean for float input.
+OPE_HD float split_level(double total, int n, bool integer) {
+    const double m = total / (double)n;
+    return integer ? (float)std::rint(m) : (float)m;
+}
+
+// Step C: write spec = x - c with replicated edges.
+template <int N>
+OPE_HD void phase_split_store(int t, const float2* vals, float2 c, float2* spec) {
+    constexpr int T = Plan<N>::T;
+    int idx = 0;
+#pragma unroll
+    for (int ch = t; ch < N / 8; ch += T, ++idx) {
+        float2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = sub2(vals[8 * idx + k], c);
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            OPE_SMEM_CHECK(SPEC_PAD + 8 * ch + i + 1 < N + 2 * SPEC_PAD);
+            *reinterpret_cast<float4*>(&spec[SPEC_PAD + 8 * ch + i]) =
+                make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
+        }
+        if (ch == 0)
+            for (int k = 0; k < SPEC_PAD; ++k) spec[k] = v[0];
+        if (ch == N / 8 - 1)
+            for (int k = 0; k < SPEC_PAD; ++k) spec[SPEC_PAD + N + k] = v[7];
+    }
+}
+
 // Rolling-average DC removal (cpu_kernels.tpp:56-82): x[i] -= mean of
 // x[i-(W-1) .. min(i+W, N-1)]. Window sums come from exact integer prefix sums
 // (the reference accumulates them in float; for integer input whose running
@@ -312,6 +369,7 @@ OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InT
 template <int N, int INTERP>
 OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v) {
     constexpr int T = Plan<N>::T;
+    const float2 NZ = dup2(a.neg_zero);
 #pragma unroll
     for (int s = 0; s < 16; ++s) {
         const int j = t + s * T;
@@ -325,7 +383,7 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
             float2 y1 = spec[e.x];
             float2 y2 = spec[e.x + 1];
             const float fr = bits_f(e.y);
-            y = add2(y1, mul2(sub2(y2, y1), dup2(fr)));
+            y = add2(y1, mul2x(sub2(y2, y1), dup2(fr), NZ));
         } else if (INTERP == INTERP_CUBIC) {
             // kLinearizationCubic + cubicHermiteInterpolation (cpu_kernels.tpp:124-145,486-502)
             int4 e = a.cub[j];
@@ -333,11 +391,13 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
             OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 < N + 2 * SPEC_PAD && i2 < N + 2 * SPEC_PAD && i3 < N + 2 * SPEC_PAD);
             const float pos = bits_f(e.z), pos2 = bits_f(e.w);
             float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i2], y3 = spec[i3];
-            float2 ca = add2(sub2(mul2(dup2(3.0f), sub2(y1, y2)), y0), y3);
-            float2 cb = sub2(add2(sub2(mul2(dup2(2.0f), y0), mul2(dup2(5.0f), y1)), mul2(dup2(4.0f), y2)), y3);
+            float2 ca = add2(sub2(mul2x(dup2(3.0f), sub2(y1, y2), NZ), y0), y3);
+            float2 cb = sub2(add2(sub2(mul2x(dup2(2.0f), y0, NZ), mul2x(dup2(5.0f), y1, NZ)),
+                                  mul2x(dup2(4.0f), y2, NZ)),
+                             y3);
             float2 cc = sub2(y2, y0);
-            float2 in = add2(add2(mul2(ca, dup2(pos2)), mul2(cb, dup2(pos))), cc);
-            y = add2(mul2(dup2(fmul_rn(0.5f, pos)), in), y1);
+            float2 in = add2(add2(mul2x(ca, dup2(pos2), NZ), mul2x(cb, dup2(pos), NZ)), cc);
+            y = add2(mul2x(dup2(fmul_rn(0.5f, pos)), in, NZ), y1);
         } else {
             // kLinearizationLanczos (cpu_kernels.tpp:176-195): sequential 16-tap sum
             int b = a.lz_base[j];
@@ -350,7 +410,7 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
 #else
                 float w = a.lz_w[k * N + j];
 #endif
-                acc = add2(acc, mul2(spec[b + k], dup2(w)));
+                acc = add2(acc, mul2x(spec[b + k], dup2(w), NZ));
             }
             y = acc;
         }
@@ -362,7 +422,7 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
         float4 q = a.wph[j];
 #endif
         float2 yw = mul2(y, dup2(q.x));
-        v[s] = cpmake(mul2(yw, dup2(q.y)), mul2(yw, dup2(q.z)));
+        v[s] = cpmake(mul2x(yw, dup2(q.y), NZ), mul2x(yw, dup2(q.z), NZ));
     }
 }
 
@@ -474,15 +534,26 @@ struct LastInfo {
     OPE_HD static int bin(int t, int i, int q) { return t + i * Plan<N>::T + q * (N / R); }
 };
 
+// Adds back the split-off DC level: X[b] += c * dc_resp[b] (both lanes).
+OPE_HD cp add_dc(const ChainArgs& a, cp x, int bin, float2 c) {
+    if (!a.dc_resp) return x;
+#if defined(__CUDA_ARCH__)
+    const float2 d = __ldg(a.dc_resp + bin);
+#else
+    const float2 d = a.dc_resp[bin];
+#endif
+    return cpmake(fma2(c, dup2(d.x), x.re), fma2(c, dup2(d.y), x.im));
+}
+
 // |X|^2 with the optional fixed-pattern subtraction (cpu_kernels.tpp:460-479).
 template <int N>
-OPE_HD void epi_mag2(int t, const cp* v, const ChainArgs& a, float2* mag2) {
+OPE_HD void epi_mag2(int t, const cp* v, const ChainArgs& a, float2 c, float2* mag2) {
     using L = LastInfo<N>;
 #pragma unroll
     for (int i = 0; i < L::D; ++i)
 #pragma unroll
         for (int q = 0; q < L::R / 2; ++q) {
-            cp x = v[i + q * L::D];
+            cp x = add_dc(a, v[i + q * L::D], L::bin(t, i, q), c);
             if (a.fpn) {
                 int b = L::bin(t, i, q);
 #if defined(__CUDA_ARCH__)

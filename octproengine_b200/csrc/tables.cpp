@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <utility>
 
 namespace ope_b200 {
 
@@ -100,6 +101,61 @@ void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std:
         if (b > n + 7) b = n + 7;
         base[j] = b - 7 + SPEC_PAD;
     }
+}
+
+namespace {
+
+// In-place iterative radix-2 inverse DFT (exp(+i)), unnormalised, float64.
+void idft_inplace(std::vector<double>& re, std::vector<double>& im) {
+    const size_t n = re.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            std::swap(re[i], re[j]);
+            std::swap(im[i], im[j]);
+        }
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const size_t half = len / 2;
+        for (size_t k = 0; k < half; ++k) {
+            const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(k) / static_cast<double>(len);
+            const double wr = std::cos(ang), wi = std::sin(ang);
+            for (size_t b = 0; b < n; b += len) {
+                const size_t i0 = b + k, i1 = b + k + half;
+                const double tr = re[i1] * wr - im[i1] * wi;
+                const double ti = re[i1] * wi + im[i1] * wr;
+                re[i1] = re[i0] - tr;
+                im[i1] = im[i0] - ti;
+                re[i0] += tr;
+                im[i0] += ti;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w, const float* window,
+                                      const float* cos_sin) {
+    std::vector<double> re(n), im(n);
+    for (int j = 0; j < n; ++j) {
+        double g = 1.0;
+        if (interp == INTERP_LANCZOS && lanczos_w) {
+            g = 0.0;
+            for (int k = 0; k < 16; ++k) g += static_cast<double>(lanczos_w[static_cast<size_t>(k) * n + j]);
+        }
+        const double w = window ? static_cast<double>(window[j]) : 1.0;
+        const double c = cos_sin ? static_cast<double>(cos_sin[2 * j]) : 1.0;
+        const double s = cos_sin ? static_cast<double>(cos_sin[2 * j + 1]) : 0.0;
+        re[j] = g * w * c;
+        im[j] = g * w * s;
+    }
+    idft_inplace(re, im);
+    std::vector<float2> d(n / 2);
+    for (int k = 0; k < n / 2; ++k) d[k] = make_float2(static_cast<float>(re[k]), static_cast<float>(im[k]));
+    return d;
 }
 
 std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n) {

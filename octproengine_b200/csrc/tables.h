@@ -28,6 +28,13 @@ std::vector<int4> build_cubic_table(const float* curve, int n);
 // first gathered index (+ SPEC_PAD) and 16 weights (tap-major, 16 x n).
 void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std::vector<float>& w);
 
+// Response of the chain up to the inverse DFT to a constant spectrum of 1:
+// D[k] = sum_j g_j w_j (cos_j + i sin_j) exp(+2 pi i j k / N), k < N/2,
+// in float64 (g_j = 1 for no/linear/cubic resampling, the sum of the 16
+// Lanczos weights of output j otherwise). Used by the exact DC split.
+std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w, const float* window,
+                                      const float* cos_sin);
+
 // {window, cos, sin, 0}; a missing window is 1, a missing phase (cos 1, sin 0).
 std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n);
 

@@ -31,6 +31,7 @@ struct EmuArgs {
     int log_scaling;
     float gmin, gmax, addend, mult;
     int flip, ascans_per_bscan, bscans;
+    int dc_split;
 };
 }
 
@@ -56,6 +57,9 @@ int emu_run(const EmuArgs& e, int what, float* out) {
     if (INTERP == INTERP_CUBIC) cub = build_cubic_table(e.curve, N);
     if (INTERP == INTERP_LANCZOS) build_lanczos_table(e.curve, N, lzb, lzw);
     std::vector<float4> wph = build_window_phase(e.window, e.cos_sin, N);
+    std::vector<float2> dcr;
+    if (e.dc_split && e.dc_window == 0)
+        dcr = build_dc_response(N, INTERP, lzw.empty() ? nullptr : lzw.data(), e.window, e.cos_sin);
 
     ChainArgs a{};
     a.in = e.in;
@@ -72,6 +76,8 @@ int emu_run(const EmuArgs& e, int what, float* out) {
     a.flip = e.flip;
     a.ascans_per_bscan = e.ascans_per_bscan;
     a.bscans = e.bscans;
+    a.neg_zero = -0.0f;
+    a.dc_resp = dcr.empty() ? nullptr : dcr.data();
 
     std::vector<unsigned char> work(LY::WORK_BYTES + 64, 0);
     std::vector<unsigned char> stage(LY::STAGE_BYTES, 0);
@@ -86,16 +92,64 @@ int emu_run(const EmuArgs& e, int what, float* out) {
         const bool has_b = r + 1 < e.m;
         std::memcpy(stage.data(), in + r * row_bytes, row_bytes * (has_b ? 2 : 1));
         if (!has_b) std::memset(stage.data() + row_bytes, 0, row_bytes);
-        if (e.dc_window > 0) {
+        float2 dc = make_float2(0.0f, 0.0f);
+        if (e.dc_window == 0 && a.dc_resp) {
+            // same reduction tree as team_sum2: xor butterfly per warp, lane 0, then warps in order
+            std::vector<std::array<float2, 16>> vals(T);
+            std::vector<double> sa(T), sb(T);
+            for (int t = 0; t < T; ++t) phase_split_load<N, DT>(t, stage.data(), vals[t].data(), &sa[t], &sb[t]);
+            double ta = 0.0, tb = 0.0;
+            for (int w = 0; w < T / 32; ++w) {
+                std::array<double, 32> xa, xb;
+                for (int l = 0; l < 32; ++l) {
+                    xa[l] = sa[32 * w + l];
+                    xb[l] = sb[32 * w + l];
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    std::array<double, 32> ya = xa, yb = xb;
+                    for (int l = 0; l < 32; ++l) {
+                        ya[l] = xa[l] + xa[l ^ o];
+                        yb[l] = xb[l] + xb[l ^ o];
+                    }
+                    xa = ya;
+                    xb = yb;
+                }
+                ta += xa[0];
+                tb += xb[0];
+            }
+            dc = make_float2(split_level(ta, N, DT != IN_F32), split_level(tb, N, DT != IN_F32));
+            for (int t = 0; t < T; ++t) phase_split_store<N>(t, vals[t].data(), dc, spec);
+        } else if (e.dc_window > 0) {
             std::vector<sum_t> ta(T), tb(T);
             for (int t = 0; t < T; ++t) phase_dc_local<N, DT>(t, stage.data(), &ta[t], &tb[t]);
-            sum_t ea = 0, eb = 0;
-            for (int t = 0; t < T; ++t) {
-                sum_t xa = ta[t], xb = tb[t];
-                ta[t] = ea;
-                tb[t] = eb;
-                ea += xa;
-                eb += xb;
+            // same order as team_exclusive_scan2: Hillis-Steele inclusive scan per
+            // warp (shfl_up by 1, 2, 4, 8, 16), warp totals added in warp order
+            {
+                std::vector<sum_t> ia(ta), ib(tb);
+                for (int w = 0; w < T / 32; ++w)
+                    for (int o = 1; o < 32; o <<= 1) {
+                        std::vector<sum_t> na(ia.begin() + 32 * w, ia.begin() + 32 * w + 32);
+                        std::vector<sum_t> nb(ib.begin() + 32 * w, ib.begin() + 32 * w + 32);
+                        for (int l = o; l < 32; ++l) {
+                            na[l] = ia[32 * w + l] + ia[32 * w + l - o];
+                            nb[l] = ib[32 * w + l] + ib[32 * w + l - o];
+                        }
+                        for (int l = 0; l < 32; ++l) {
+                            ia[32 * w + l] = na[l];
+                            ib[32 * w + l] = nb[l];
+                        }
+                    }
+                for (int t = 0; t < T; ++t) {
+                    const int w = t / 32;
+                    sum_t pa = 0, pb = 0;
+                    for (int u = 0; u < w; ++u) {
+                        pa += ia[32 * u + 31];
+                        pb += ib[32 * u + 31];
+                    }
+                    const sum_t xa = ta[t], xb = tb[t];
+                    ta[t] = pa + ia[t] - xa;
+                    tb[t] = pb + ib[t] - xb;
+                }
             }
             for (int t = 0; t < T; ++t) phase_dc_prefix<N, DT>(t, stage.data(), ta[t], tb[t], pfx);
             for (int t = 0; t < T; ++t) phase_dc_apply<N, DT>(t, stage.data(), pfx, e.dc_window, spec);
@@ -143,7 +197,11 @@ int emu_run(const EmuArgs& e, int what, float* out) {
                 for (int i = 0; i < L::D; ++i)
                     for (int q = 0; q < L::R / 2; ++q) {
                         const int bin = L::bin(t, i, q);
-                        const cp x = v[t][i + q * L::D];
+                        cp x = add_dc(a, v[t][i + q * L::D], bin, dc);
+                        if (a.fpn) {
+                            x.re = sub2(x.re, dup2(a.fpn[bin].x));
+                            x.im = sub2(x.im, dup2(a.fpn[bin].y));
+                        }
                         out[(r * (N / 2) + bin) * 2] = x.re.x;
                         out[(r * (N / 2) + bin) * 2 + 1] = x.im.x;
                         if (has_b) {
@@ -157,7 +215,7 @@ int emu_run(const EmuArgs& e, int what, float* out) {
         std::vector<float> img(2 * (N / 2));
         for (int t = 0; t < T; ++t) {
             float2 mag2[L::NB];
-            epi_mag2<N>(t, v[t].data(), a, mag2);
+            epi_mag2<N>(t, v[t].data(), a, dc, mag2);
             for (int i = 0; i < L::D; ++i)
                 for (int q = 0; q < L::R / 2; ++q) {
                     const int bin = L::bin(t, i, q);

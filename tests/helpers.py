@@ -27,7 +27,8 @@ class EmuArgs(ctypes.Structure):
                 ("window", ctypes.c_void_p), ("cos_sin", ctypes.c_void_p), ("fpn", ctypes.c_void_p),
                 ("dc_window", ctypes.c_int), ("log_scaling", ctypes.c_int), ("gmin", ctypes.c_float),
                 ("gmax", ctypes.c_float), ("addend", ctypes.c_float), ("mult", ctypes.c_float),
-                ("flip", ctypes.c_int), ("ascans_per_bscan", ctypes.c_int), ("bscans", ctypes.c_int)]
+                ("flip", ctypes.c_int), ("ascans_per_bscan", ctypes.c_int), ("bscans", ctypes.c_int),
+                ("dc_split", ctypes.c_int)]
 
 
 def emu_lib():
@@ -59,7 +60,7 @@ def emu_run(L, spec: ChainSpec, raw: np.ndarray, what: str = "image", fpn=None) 
                 _ptr(cs) if spec.dispersion else None, _ptr(fp),
                 spec.dc_window if spec.dc_removal else 0, int(spec.log_scaling), spec.grayscale_min,
                 spec.grayscale_max, spec.addend, spec.multiplicator, int(spec.bscan_flip),
-                spec.ascans_per_bscan, spec.bscans_per_buffer)
+                spec.ascans_per_bscan, spec.bscans_per_buffer, int(spec.dc_split))
     code = {"image": 0, "fft_input": 1, "bins": 2}[what]
     if what == "image":
         out = np.zeros((m, n // 2), np.float32)
