@@ -96,8 +96,8 @@ __device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
 
 // Team sum of two doubles, in a fixed order (xor butterfly inside each warp,
 // then warp totals in warp order) that the CPU emulation reproduces.
-template <int T>
-__device__ __forceinline__ void team_sum2(double& a, double& b, double* scratch) {
+template <int T, typename S>
+__device__ __forceinline__ void team_sum2(S& a, S& b, S* scratch) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -109,7 +109,7 @@ __device__ __forceinline__ void team_sum2(double& a, double& b, double* scratch)
         scratch[2 * warp + 1] = b;
     }
     __syncthreads();
-    double ta = 0.0, tb = 0.0;
+    S ta = 0, tb = 0;
     for (int w = 0; w < T / 32; ++w) {
         ta += scratch[2 * w];
         tb += scratch[2 * w + 1];
@@ -273,11 +273,12 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
             __syncthreads();
             phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
         } else if (a.dc_resp) {
+            using SS = typename SplitSum<DT>::type;
             float2 vals[16];
-            double sa, sb;
+            SS sa, sb;
             phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
-            team_sum2<T>(sa, sb, reinterpret_cast<double*>(scan));
-            dc = make_float2(split_level(sa, N, DT != IN_F32), split_level(sb, N, DT != IN_F32));
+            team_sum2<T, SS>(sa, sb, reinterpret_cast<SS*>(scan));
+            dc = make_float2(split_level((double)sa, N, DT != IN_F32), split_level((double)sb, N, DT != IN_F32));
             phase_split_store<N>(t, vals, dc, spec);
         } else {
             phase_unpack<N, DT>(t, stage, spec);
@@ -342,7 +343,7 @@ struct ImageSink {
 };
 
 template <int N, int DT, int INTERP>
-__global__ void __launch_bounds__(N / 16) chain_kernel(const ChainArgs a) {
+__global__ void __launch_bounds__(N / 16, 3) chain_kernel(const ChainArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     using LY = Layout<N, DT>;
     ImageSink<N> sink{a, reinterpret_cast<float*>(smem + LY::OFF_SCAN)};

@@ -57,7 +57,7 @@ struct ChainArgs {
     const int4* cub;     // CUBIC: {n0|n1<<16, n2|n3<<16 (all +PAD), pos bits, pos^2 bits}
     const int* lz_base;  // LANCZOS: first tap index + PAD
     const float* lz_w;   // LANCZOS: 16 x N tap weights, tap-major
-    const float4* wph;   // {window, cos(phase), sin(phase), 0}
+    const float4* wph;   // {w*cos, w*cos, w*sin, w*sin} (window folded into the phase)
     const float2* fpn;   // N/2 complex fixed-pattern profile, or nullptr
     int dc_window;       // rolling-average half window W; 0 = off
     int log_mode;        // 1: logarithmic, 0: linear
@@ -78,6 +78,7 @@ struct ChainArgs {
     // evaluated in float64; the chain is linear up to the DFT, so the result
     // is the same quantity computed with a far smaller float32 error floor.
     const float2* dc_resp;
+    float* resampled_out;  // test hook (CPU emulation only): k-linearised spectrum of the last pair
 };
 
 template <int N_>
@@ -210,45 +211,103 @@ OPE_HD void load_raw_pair(const unsigned char* stage, int n, int i, typename InT
     sb = (sum_t)ra[n + i];
 }
 
+// Samples 2p and 2p+1 of both rows: out[0] = (a[2p], b[2p]), out[1] = (a[2p+1], b[2p+1]).
+template <int DT>
+OPE_HD void load_pos2(const unsigned char* stage, int n, int p, float2* out) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    const raw_t* ra = reinterpret_cast<const raw_t*>(stage);
+    const raw_t* rb = ra + n;
+#if defined(__CUDA_ARCH__)
+    if (DT == IN_U16) {
+        const unsigned wa = *reinterpret_cast<const unsigned*>(ra + 2 * p);
+        const unsigned wb = *reinterpret_cast<const unsigned*>(rb + 2 * p);
+        const float2 magic = dup2(8388608.0f);
+        out[0] = sub2(make_float2(__uint_as_float(__byte_perm(wa, 0x4B00u, 0x5410)),
+                                  __uint_as_float(__byte_perm(wb, 0x4B00u, 0x5410))), magic);
+        out[1] = sub2(make_float2(__uint_as_float(__byte_perm(wa, 0x4B00u, 0x5432)),
+                                  __uint_as_float(__byte_perm(wb, 0x4B00u, 0x5432))), magic);
+        return;
+    }
+    if (DT == IN_U8) {
+        const unsigned wa = *reinterpret_cast<const unsigned short*>(ra + 2 * p);
+        const unsigned wb = *reinterpret_cast<const unsigned short*>(rb + 2 * p);
+        const float2 magic = dup2(8388608.0f);
+        out[0] = sub2(make_float2(__uint_as_float(__byte_perm(wa, 0x4B00u, 0x5440)),
+                                  __uint_as_float(__byte_perm(wb, 0x4B00u, 0x5440))), magic);
+        out[1] = sub2(make_float2(__uint_as_float(__byte_perm(wa, 0x4B00u, 0x5441)),
+                                  __uint_as_float(__byte_perm(wb, 0x4B00u, 0x5441))), magic);
+        return;
+    }
+#endif
+    for (int i = 0; i < 2; ++i) {
+        const raw_t a = ra[2 * p + i], b = rb[2 * p + i];
+        if (DT == IN_U32) {
+#if defined(__CUDA_ARCH__)
+            out[i] = make_float2(__uint2float_rn((unsigned)a), __uint2float_rn((unsigned)b));
+#else
+            out[i] = make_float2((float)(unsigned)a, (float)(unsigned)b);
+#endif
+        } else {
+            out[i] = make_float2((float)a, (float)b);
+        }
+    }
+}
+
 // Plain unpack (no DC removal): spec[PAD + k] = (a[k], b[k]) for k < N, with
-// replicated edges. Thread t handles chunks c = t, t + T (8 samples each).
+// replicated edges. Thread t handles the sample pairs p = t + k*T (k < 8),
+// i.e. samples 2p and 2p+1: consecutive lanes read consecutive 32-bit raw
+// words and write consecutive 16-byte spec slots (no bank conflicts).
 template <int N, int DT>
 OPE_HD void phase_unpack(int t, const unsigned char* stage, float2* spec) {
     constexpr int T = Plan<N>::T;
 #pragma unroll
-    for (int c = t; c < N / 8; c += T) {
-        float2 v[8];
-        load_chunk8<DT>(stage, N, c, v);
-#pragma unroll
-        for (int i = 0; i < 8; i += 2) {
-            OPE_SMEM_CHECK(SPEC_PAD + 8 * c + i + 1 < N + 2 * SPEC_PAD);
-            *reinterpret_cast<float4*>(&spec[SPEC_PAD + 8 * c + i]) =
-                make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
-        }
-        if (c == 0) {
-            for (int k = 0; k < SPEC_PAD; ++k) spec[k] = v[0];
-        }
-        if (c == N / 8 - 1) {
-            for (int k = 0; k < SPEC_PAD; ++k) spec[SPEC_PAD + N + k] = v[7];
-        }
+    for (int k = 0; k < 8; ++k) {
+        const int p = t + k * T;
+        float2 v[2];
+        load_pos2<DT>(stage, N, p, v);
+        OPE_SMEM_CHECK(SPEC_PAD + 2 * p + 1 < N + 2 * SPEC_PAD);
+        *reinterpret_cast<float4*>(&spec[SPEC_PAD + 2 * p]) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+        if (p == 0)
+            for (int e = 0; e < SPEC_PAD; ++e) spec[e] = v[0];
+        if (p == N / 2 - 1)
+            for (int e = 0; e < SPEC_PAD; ++e) spec[SPEC_PAD + N + e] = v[1];
     }
 }
 
 // Exact DC split, step A: thread t loads its two 8-sample chunks (kept in
 // registers across the team reduction) and sums each row in double.
+// Sum type of the split level: exact integers for 8/16-bit samples (at most
+// 8192 * 65535 < 2^31), double otherwise.
+template <int DT>
+struct SplitSum { using type = double; };
+template <>
+struct SplitSum<IN_U8> { using type = int; };
+template <>
+struct SplitSum<IN_U16> { using type = int; };
+
 template <int N, int DT>
-OPE_HD void phase_split_load(int t, const unsigned char* stage, float2* vals, double* sa, double* sb) {
+OPE_HD void phase_split_load(int t, const unsigned char* stage, float2* vals, typename SplitSum<DT>::type* sa,
+                             typename SplitSum<DT>::type* sb) {
+    using S = typename SplitSum<DT>::type;
     constexpr int T = Plan<N>::T;
-    double a = 0.0, b = 0.0;
-    int idx = 0;
+    float fa = 0.0f, fb = 0.0f;  // exact: 16 samples below 2^16 sum below 2^24
+    S a = 0, b = 0;
 #pragma unroll
-    for (int c = t; c < N / 8; c += T, ++idx) {
-        load_chunk8<DT>(stage, N, c, vals + 8 * idx);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            a += (double)vals[8 * idx + k].x;
-            b += (double)vals[8 * idx + k].y;
+    for (int k = 0; k < 8; ++k) {
+        load_pos2<DT>(stage, N, t + k * T, vals + 2 * k);
+        if (DT == IN_U8 || DT == IN_U16) {
+            fa = fadd_rn(fadd_rn(fa, vals[2 * k].x), vals[2 * k + 1].x);
+            fb = fadd_rn(fadd_rn(fb, vals[2 * k].y), vals[2 * k + 1].y);
+        } else {
+            a += (S)vals[2 * k].x;
+            b += (S)vals[2 * k].y;
+            a += (S)vals[2 * k + 1].x;
+            b += (S)vals[2 * k + 1].y;
         }
+    }
+    if (DT == IN_U8 || DT == IN_U16) {
+        a = (S)fa;
+        b = (S)fb;
     }
     *sa = a;
     *sb = b;
@@ -265,22 +324,16 @@ OPE_HD float split_level(double total, int n, bool integer) {
 template <int N>
 OPE_HD void phase_split_store(int t, const float2* vals, float2 c, float2* spec) {
     constexpr int T = Plan<N>::T;
-    int idx = 0;
 #pragma unroll
-    for (int ch = t; ch < N / 8; ch += T, ++idx) {
-        float2 v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = sub2(vals[8 * idx + k], c);
-#pragma unroll
-        for (int i = 0; i < 8; i += 2) {
-            OPE_SMEM_CHECK(SPEC_PAD + 8 * ch + i + 1 < N + 2 * SPEC_PAD);
-            *reinterpret_cast<float4*>(&spec[SPEC_PAD + 8 * ch + i]) =
-                make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
-        }
-        if (ch == 0)
-            for (int k = 0; k < SPEC_PAD; ++k) spec[k] = v[0];
-        if (ch == N / 8 - 1)
-            for (int k = 0; k < SPEC_PAD; ++k) spec[SPEC_PAD + N + k] = v[7];
+    for (int k = 0; k < 8; ++k) {
+        const int p = t + k * T;
+        const float2 v0 = sub2(vals[2 * k], c), v1 = sub2(vals[2 * k + 1], c);
+        OPE_SMEM_CHECK(SPEC_PAD + 2 * p + 1 < N + 2 * SPEC_PAD);
+        *reinterpret_cast<float4*>(&spec[SPEC_PAD + 2 * p]) = make_float4(v0.x, v0.y, v1.x, v1.y);
+        if (p == 0)
+            for (int e = 0; e < SPEC_PAD; ++e) spec[e] = v0;
+        if (p == N / 2 - 1)
+            for (int e = 0; e < SPEC_PAD; ++e) spec[SPEC_PAD + N + e] = v1;
     }
 }
 
@@ -414,15 +467,22 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
             }
             y = acc;
         }
-        // applyWindow then dispersionCompensation (cpu_kernels.tpp:198-235):
-        // re = (y*w)*cos, im = (y*w)*sin
-#if defined(__CUDA_ARCH__)
-        float4 q = __ldg(a.wph + j);
-#else
-        float4 q = a.wph[j];
+#if !defined(__CUDA_ARCH__)
+        if (a.resampled_out) {  // CPU emulation only: the k-linearised spectrum of this pair
+            a.resampled_out[(long long)j * 2] = y.x;
+            a.resampled_out[(long long)j * 2 + 1] = y.y;
+        }
 #endif
-        float2 yw = mul2(y, dup2(q.x));
-        v[s] = cpmake(mul2x(yw, dup2(q.y), NZ), mul2x(yw, dup2(q.z), NZ));
+        // applyWindow then dispersionCompensation (cpu_kernels.tpp:198-235):
+        // re = y*w*cos, im = y*w*sin with the window folded into the phase
+        // factors (w*cos, w*sin), evaluated in double and rounded once; the
+        // table holds each factor twice, one per lane.
+#if defined(__CUDA_ARCH__)
+        const float4 q = __ldg(a.wph + j);
+#else
+        const float4 q = a.wph[j];
+#endif
+        v[s] = cpmake(mul2x(y, make_float2(q.x, q.y), NZ), mul2x(y, make_float2(q.z, q.w), NZ));
     }
 }
 
@@ -439,6 +499,11 @@ struct PassInfo {
     static constexpr int R = LAST ? Plan<N>::LASTR : 16;
     static constexpr int D = 16 / R;
     static constexpr int NS = (P == 0) ? 1 : (P == 1) ? 16 : (P == 2) ? 256 : 4096;
+    // Twiddles of pass P >= 1 live in one block of (R-1) x NS entries,
+    // entry (r-1)*NS + k = W_{NS*R}^{r*k}: threads with consecutive k read
+    // consecutive entries. Blocks of successive passes follow each other.
+    static constexpr int TW_SIZE = (P == 0) ? 0 : (R - 1) * NS;
+    static constexpr int TW_OFF = (P <= 1) ? 0 : PassInfo<N, (P > 1 ? P - 1 : 0)>::TW_OFF + PassInfo<N, (P > 1 ? P - 1 : 0)>::TW_SIZE;
 };
 
 template <int N>
@@ -467,10 +532,9 @@ OPE_HD void fft_twiddle_dft(int t, cp* v, const float2* tw) {
         if (P > 0) {
             const int d = t + i * T;
             const int k = d % NS;
-            const int stride = N / (NS * R);
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                const int idx = r * k * stride;
+                const int idx = PI::TW_OFF + (r - 1) * NS + k;
                 OPE_SMEM_CHECK(idx >= 0 && idx < N);
 #if defined(__CUDA_ARCH__)
                 float2 w = __ldg(tw + idx);

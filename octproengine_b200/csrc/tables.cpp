@@ -38,10 +38,28 @@ float lanczos8(float x) {
 }
 
 std::vector<float2> build_twiddles(int n) {
-    std::vector<float2> tw(n);
-    for (int j = 0; j < n; ++j) {
-        const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(j) / n;
-        tw[j] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
+    // Per Stockham pass p >= 1 (radix R, span NS): (R-1) x NS entries,
+    // entry (r-1)*NS + k = W_N^(r k N/(NS R)), matching PassInfo::TW_OFF.
+    std::vector<float2> tw(n, make_float2(1.0f, 0.0f));
+    int log2n = 0;
+    while ((1 << log2n) < n) ++log2n;
+    const int npass = (log2n + 3) / 4;
+    const int lastr = 1 << (log2n - 4 * (npass - 1));
+    int off = 0, ns = 1;
+    for (int p = 0; p < npass; ++p) {
+        const int r_p = (p == npass - 1) ? lastr : 16;
+        if (p > 0) {
+            const int stride = n / (ns * r_p);
+            for (int r = 1; r < r_p; ++r)
+                for (int k = 0; k < ns; ++k) {
+                    const long long j = static_cast<long long>(r) * k * stride;
+                    const double ang = 2.0 * 3.14159265358979323846 * static_cast<double>(j) / n;
+                    tw[off + (r - 1) * ns + k] =
+                        make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
+                }
+            off += (r_p - 1) * ns;
+        }
+        ns *= r_p;
     }
     return tw;
 }
@@ -160,9 +178,12 @@ std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w,
 
 std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n) {
     std::vector<float4> t(n);
-    for (int j = 0; j < n; ++j)
-        t[j] = make_float4(window ? window[j] : 1.0f, cos_sin ? cos_sin[2 * j] : 1.0f,
-                           cos_sin ? cos_sin[2 * j + 1] : 0.0f, 0.0f);
+    for (int j = 0; j < n; ++j) {
+        const double w = window ? static_cast<double>(window[j]) : 1.0;
+        const float wc = static_cast<float>(w * (cos_sin ? static_cast<double>(cos_sin[2 * j]) : 1.0));
+        const float ws = static_cast<float>(w * (cos_sin ? static_cast<double>(cos_sin[2 * j + 1]) : 0.0));
+        t[j] = make_float4(wc, wc, ws, ws);
+    }
     return t;
 }
 

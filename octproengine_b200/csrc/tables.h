@@ -13,7 +13,8 @@ namespace ope_b200 {
 // evaluated with the same float operations.
 float lanczos8(float x);
 
-// W_N^j = exp(+2 pi i j / N), j < N, evaluated in double and rounded once.
+// Twiddles of the Stockham passes, per pass a block of (R-1) x NS entries
+// W_N^(r k N/(NS R)) (see PassInfo::TW_OFF), evaluated in double and rounded once.
 std::vector<float2> build_twiddles(int n);
 
 // kLinearizationLinear indices and fractions (cpu_kernels.tpp:95-110):
@@ -35,7 +36,9 @@ void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std:
 std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w, const float* window,
                                       const float* cos_sin);
 
-// {window, cos, sin, 0}; a missing window is 1, a missing phase (cos 1, sin 0).
+// {w cos, w cos, w sin, w sin} per sample (each factor once per lane of a
+// pair), products in double rounded once; a missing window is 1, a missing
+// phase (cos 1, sin 0).
 std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n);
 
 // Output affine constants of logScaleAndTruncate / linearScaleAndTruncate

@@ -37,7 +37,7 @@ struct EmuArgs {
 
 namespace {
 
-enum { OUT_IMAGE = 0, OUT_FFT_INPUT = 1, OUT_BINS = 2 };
+enum { OUT_IMAGE = 0, OUT_FFT_INPUT = 1, OUT_BINS = 2, OUT_RESAMPLED = 3 };
 
 template <int N, int DT, int INTERP>
 int emu_run(const EmuArgs& e, int what, float* out) {
@@ -95,18 +95,19 @@ int emu_run(const EmuArgs& e, int what, float* out) {
         float2 dc = make_float2(0.0f, 0.0f);
         if (e.dc_window == 0 && a.dc_resp) {
             // same reduction tree as team_sum2: xor butterfly per warp, lane 0, then warps in order
+            using SS = typename SplitSum<DT>::type;
             std::vector<std::array<float2, 16>> vals(T);
-            std::vector<double> sa(T), sb(T);
+            std::vector<SS> sa(T), sb(T);
             for (int t = 0; t < T; ++t) phase_split_load<N, DT>(t, stage.data(), vals[t].data(), &sa[t], &sb[t]);
-            double ta = 0.0, tb = 0.0;
+            SS ta = 0, tb = 0;
             for (int w = 0; w < T / 32; ++w) {
-                std::array<double, 32> xa, xb;
+                std::array<SS, 32> xa, xb;
                 for (int l = 0; l < 32; ++l) {
                     xa[l] = sa[32 * w + l];
                     xb[l] = sb[32 * w + l];
                 }
                 for (int o = 16; o > 0; o >>= 1) {
-                    std::array<double, 32> ya = xa, yb = xb;
+                    std::array<SS, 32> ya = xa, yb = xb;
                     for (int l = 0; l < 32; ++l) {
                         ya[l] = xa[l] + xa[l ^ o];
                         yb[l] = xb[l] + xb[l ^ o];
@@ -117,7 +118,7 @@ int emu_run(const EmuArgs& e, int what, float* out) {
                 ta += xa[0];
                 tb += xb[0];
             }
-            dc = make_float2(split_level(ta, N, DT != IN_F32), split_level(tb, N, DT != IN_F32));
+            dc = make_float2(split_level((double)ta, N, DT != IN_F32), split_level((double)tb, N, DT != IN_F32));
             for (int t = 0; t < T; ++t) phase_split_store<N>(t, vals[t].data(), dc, spec);
         } else if (e.dc_window > 0) {
             std::vector<sum_t> ta(T), tb(T);
@@ -156,7 +157,20 @@ int emu_run(const EmuArgs& e, int what, float* out) {
         } else {
             for (int t = 0; t < T; ++t) phase_unpack<N, DT>(t, stage.data(), spec);
         }
+        std::vector<float> rs;
+        if (what == OUT_RESAMPLED) {
+            rs.assign(2 * N, 0.0f);
+            a.resampled_out = rs.data();
+        }
         for (int t = 0; t < T; ++t) phase_prestage<N, INTERP>(t, spec, a, v[t].data());
+        a.resampled_out = nullptr;
+        if (what == OUT_RESAMPLED) {
+            for (int j = 0; j < N; ++j) {
+                out[r * N + j] = rs[2 * j];
+                if (has_b) out[(r + 1) * N + j] = rs[2 * j + 1];
+            }
+            continue;
+        }
         if (what == OUT_FFT_INPUT) {
             for (int t = 0; t < T; ++t)
                 for (int s = 0; s < 16; ++s) {

@@ -61,7 +61,11 @@ def emu_run(L, spec: ChainSpec, raw: np.ndarray, what: str = "image", fpn=None) 
                 spec.dc_window if spec.dc_removal else 0, int(spec.log_scaling), spec.grayscale_min,
                 spec.grayscale_max, spec.addend, spec.multiplicator, int(spec.bscan_flip),
                 spec.ascans_per_bscan, spec.bscans_per_buffer, int(spec.dc_split))
-    code = {"image": 0, "fft_input": 1, "bins": 2}[what]
+    code = {"image": 0, "fft_input": 1, "bins": 2, "resampled": 3}[what]
+    if what == "resampled":
+        out = np.zeros((m, n), np.float32)
+        assert L.emu_chain(ctypes.byref(e), code, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))) == 0
+        return out
     if what == "image":
         out = np.zeros((m, n // 2), np.float32)
     elif what == "fft_input":
