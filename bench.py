@@ -238,11 +238,24 @@ def run_ours(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        # nvidia-smi needs a moment to start: wait for its first sample, then
+        # keep the same work running for ~0.5 s so the sampled clocks are the
+        # clocks under this load, then time the K steps inside the sampling window
+        t_wait = time.time()
+        while not clk.lines and time.time() - t_wait < 5.0:
+            time.sleep(0.05)
+        t_soak = time.time()
+        while time.time() - t_soak < 0.5:
+            for _ in range(50):
+                ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
+            torch.cuda.synchronize(dev)
+        barrier()
         ev0.record(stream)
         for _ in range(args.steps):
             ctx.process_device(x.data_ptr(), out.data_ptr(), sp)
         ev1.record(stream)
         barrier()
+        time.sleep(0.25)
     ms = ev0.elapsed_time(ev1)
     t = torch.tensor([ms], device=dev)
     if dist is not None:
@@ -357,7 +370,7 @@ def main():
     global BSCANS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
