@@ -137,6 +137,27 @@ OPE_B200_API int ope_b200_request_fpn_determination(ope_b200_ctx* ctx);
 OPE_B200_API int ope_b200_set_fpn_profile(ope_b200_ctx* ctx, const float* interleaved, size_t complex_pairs);
 OPE_B200_API int ope_b200_get_fpn_profile(ope_b200_ctx* ctx, float* out, size_t cap_pairs, size_t* pairs);
 
+/* Fixed-pattern-noise determination that allocates nothing. No counterpart in
+ * the reference. For callers that may not allocate device memory once running:
+ * a real-time acquisition thread must not stall on cudaMalloc/cudaFree (they
+ * can synchronise the whole device), and integrations that budget all device
+ * memory at start-up may not allocate afterwards. The allocating path
+ * (request + process) grows a scratch buffer with cudaMalloc on first use; this
+ * call keeps its scratch in one static device array of 3.4 MiB, which every
+ * GPU that loads the library holds until the process exits.
+ *
+ * Computes the minimum-variance-mean profile (cpu_kernels.tpp:402-458) of the
+ * first fpn_bscan_count * ascans_per_bscan A-scans of the device buffer d_in
+ * (num_ascans A-scans, at least that many) and writes N/2 interleaved
+ * (re, im) float pairs to d_profile (8-byte aligned). Asynchronous on
+ * `stream`; the context's own FPN state is not changed. Limits: signal length
+ * up to 4096 (OPE_B200_E_UNSUPPORTED beyond). The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture. All calls share the one array: calls that overlap on the GPU race
+ * and corrupt each other's results. */
+OPE_B200_API int ope_b200_determine_fpn_noalloc(ope_b200_ctx* ctx, const void* d_in, int64_t num_ascans,
+                                                float* d_profile, void* stream);
+
 /* ---- post-process background: ProcessingBackend::requestPostProcessBackgroundRecording /
  *      set/getPostProcessBackgroundProfile (backend_interface.h:40-42) ---- */
 OPE_B200_API int ope_b200_request_bg_recording(ope_b200_ctx* ctx);

@@ -97,6 +97,7 @@ SIGNATURES = {
     "ope_b200_request_fpn_determination": (ctypes.c_int, [_P]),
     "ope_b200_set_fpn_profile": (ctypes.c_int, [_P, _FP, _SZ]),
     "ope_b200_get_fpn_profile": (ctypes.c_int, [_P, _FP, _SZ, ctypes.POINTER(_SZ)]),
+    "ope_b200_determine_fpn_noalloc": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
     "ope_b200_request_bg_recording": (ctypes.c_int, [_P]),
     "ope_b200_set_bg_profile": (ctypes.c_int, [_P, _FP, _SZ]),
     "ope_b200_get_bg_profile": (ctypes.c_int, [_P, _FP, _SZ, ctypes.POINTER(_SZ)]),
@@ -259,6 +260,11 @@ class Context:
     def set_fpn_profile(self, interleaved: np.ndarray) -> None:
         p = np.ascontiguousarray(interleaved, np.float32)
         self.check(lib().ope_b200_set_fpn_profile(self.h, fptr(p), p.size // 2))
+
+    def determine_fpn_noalloc(self, d_in: int, num_ascans: int, d_profile: int, stream: int = 0) -> None:
+        """FPN profile of the first fpn_bscan_count*A A-scans of a device buffer,
+        using the library's static scratch array (no device allocation)."""
+        self.check(lib().ope_b200_determine_fpn_noalloc(self.h, d_in, int(num_ascans), d_profile, stream))
 
     def fpn_profile(self) -> np.ndarray:
         pairs = _SZ(0)

@@ -551,3 +551,90 @@ cudaError_t launch_chain(int n, int in_kind, int interp, const ChainArgs& a, cud
 }
 
 }  // namespace ope_b200
+
+// ---------------------------------------------------------------------------
+// Fixed-pattern-noise determination without device allocation.
+//
+// Some callers cannot allocate device memory once they are running: a
+// real-time acquisition thread must not stall the frame loop (cudaMalloc and
+// cudaFree can synchronise the whole device), and integrations that budget all
+// device memory at start-up may not allocate afterwards. The allocating path
+// (ope_b200_request_fpn_determination + process) grows its partial-sum buffer
+// with cudaMalloc on first use. This variant keeps those partial sums and the
+// segment accumulators in one file-scope device array of fixed size instead.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kNoAllocMaxN = 4096;  // longest A-scan the static scratch serves
+constexpr int kNoAllocMaxGx = 8;    // CTAs per FPN segment
+constexpr size_t kNoAllocPartial = static_cast<size_t>(FPN_SEGMENTS) * kNoAllocMaxGx * (kNoAllocMaxN / 2) * 3;
+constexpr size_t kNoAllocAcc = static_cast<size_t>(FPN_SEGMENTS) * (kNoAllocMaxN / 2) * 3;
+
+// 3.4 MiB per GPU that loads the library, held until the process exits.
+static __device__ __align__(256) double g_fpn_noalloc_scratch[kNoAllocPartial + kNoAllocAcc];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device (`dev`). In host
+// code the array's name is only a host-side stand-in, never a device address.
+cudaError_t noalloc_scratch(int dev, double** out) {
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_fpn_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ope_b200_determine_fpn_noalloc(ope_b200_ctx* c, const void* d_in, int64_t num_ascans, float* d_profile,
+                                   void* stream) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!d_in || !d_profile || num_ascans < 1) return fail(c, OPE_B200_E_INVALID, "null buffer or empty A-scan count");
+    if (!aligned16(d_in)) return fail(c, OPE_B200_E_INVALID, "input buffer must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(d_profile) & 7u) != 0)
+        return fail(c, OPE_B200_E_INVALID, "profile buffer must be 8-byte aligned");
+    if (c->n > kNoAllocMaxN)
+        return fail(c, OPE_B200_E_UNSUPPORTED, "no-allocation FPN determination supports signal lengths up to " +
+                                                   std::to_string(kNoAllocMaxN));
+    const long long required = static_cast<long long>(c->cfg.fpn_bscan_count) * c->cfg.ascans_per_bscan;
+    const long long seg_w = required / FPN_SEGMENTS;
+    if (seg_w < 1) return fail(c, OPE_B200_E_INVALID, "fixed-pattern noise determination needs at least 8 A-scans");
+    if (num_ascans < required)
+        return fail(c, OPE_B200_E_INVALID, "buffer holds fewer A-scans than fpnBscanCount * ascansPerBscan");
+    OPE_CU(c, cudaSetDevice(c->device));
+    double* scratch = nullptr;
+    OPE_CU(c, noalloc_scratch(c->device, &scratch));
+    if (c->tables_dirty) {
+        int rc = rebuild_tables(c);
+        if (rc != OPE_B200_OK) return rc;
+    }
+    const long long pairs_per_seg = (seg_w + 1) / 2;
+    long long gx = (pairs_per_seg + 3) / 4;
+    if (gx < 1) gx = 1;
+    if (gx > kNoAllocMaxGx) gx = kNoAllocMaxGx;
+    const int half = c->n / 2;
+    double* partial = scratch;
+    double* acc = scratch + kNoAllocPartial;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ChainArgs a = make_args(c, d_in, nullptr, num_ascans, nullptr);
+    // the accumulators must start at zero; the partials are fully overwritten
+    OPE_CU(c, cudaMemsetAsync(acc, 0, static_cast<size_t>(FPN_SEGMENTS) * half * 3 * sizeof(double), s));
+    OPE_CU(c, launch_fpn_stats(c->n, c->in_kind, c->interp, a, 0, required, seg_w, static_cast<int>(gx), partial, s));
+    OPE_CU(c, launch_fpn_reduce(partial, acc, static_cast<int>(gx), half, s));
+    OPE_CU(c, launch_fpn_finalize(acc, reinterpret_cast<float2*>(d_profile), half, seg_w, s));
+    OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
+    return OPE_B200_OK;
+}
+
+}  // extern "C"

@@ -151,6 +151,17 @@ int fpn_get_profile(FpnState& st, float* out, size_t cap_pairs, size_t* pairs, s
     return OPE_B200_OK;
 }
 
+cudaError_t launch_fpn_reduce(const double* partial, double* acc, int gx, int half, cudaStream_t s) {
+    const int per_seg = half * 3;
+    fpn_reduce_kernel<<<dim3((per_seg + 255) / 256, FPN_SEGMENTS), 256, 0, s>>>(partial, acc, gx, per_seg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fpn_finalize(const double* acc, float2* profile, int half, long long seg_w, cudaStream_t s) {
+    fpn_finalize_kernel<<<(half + 255) / 256, 256, 0, s>>>(acc, profile, half, seg_w);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fpn_stats(int n, int in_kind, int interp, const ChainArgs& a, long long g0, long long rows,
                              long long seg_w, int gx, double* partial, cudaStream_t s) {
     switch (n) {

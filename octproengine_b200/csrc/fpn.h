@@ -46,6 +46,11 @@ int fpn_get_profile(FpnState& st, float* out, size_t cap_pairs, size_t* pairs, s
 cudaError_t launch_fpn_stats(int n, int in_kind, int interp, const ChainArgs& a, long long g0, long long rows,
                              long long seg_w, int gx, double* partial, cudaStream_t s);
 
+// Enqueue the fixed-order reduction of the per-CTA partial sums into acc
+// (acc += partials) and the minimum-variance selection into a profile.
+cudaError_t launch_fpn_reduce(const double* partial, double* acc, int gx, int half, cudaStream_t s);
+cudaError_t launch_fpn_finalize(const double* acc, float2* profile, int half, long long seg_w, cudaStream_t s);
+
 #define OPE_B200_DECLARE_FPN_N(NN)                                                                          \
     cudaError_t launch_fpn_stats_n##NN(int in_kind, int interp, const ChainArgs& a, long long g0, long long rows, \
                                        long long seg_w, int gx, double* partial, cudaStream_t s);
