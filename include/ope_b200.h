@@ -102,7 +102,8 @@ OPE_B200_API int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out)
 OPE_B200_API void ope_b200_destroy(ope_b200_ctx* ctx);
 /* ProcessingBackend::updateConfig (backend_interface.h:27): non-dimension fields only. */
 OPE_B200_API int ope_b200_update_config(ope_b200_ctx* ctx, const ope_b200_config* cfg);
-/* Last error message of this context (never NULL). */
+/* Last error message of this context (never NULL); with ctx == NULL, why the calling
+ * thread's last ope_b200_create failed. */
 OPE_B200_API const char* ope_b200_last_error(const ope_b200_ctx* ctx);
 
 /* ---- hot-swap curves: ProcessingBackend::update{Resampling,Dispersion,Window}Curve
@@ -130,6 +131,28 @@ OPE_B200_API int ope_b200_process_bins_device(ope_b200_ctx* ctx, const void* d_i
 /* Host to host, synchronous: copies h_in to the device, runs the chain, copies
  * the result to h_out and waits. */
 OPE_B200_API int ope_b200_process_host(ope_b200_ctx* ctx, const void* h_in, float* h_out);
+
+/* ---- streaming ring: the IOBuffer path of ProcessingBackend::process and
+ *      getNextAvailableInputBuffer (backend_interface.h:24,35-37).
+ *      Depth = num_input_buffers (>= 2). A frame is copied in, processed and
+ *      copied out on its own stream; neighbouring frames overlap. ---- */
+OPE_B200_API int ope_b200_ring_depth(ope_b200_ctx* ctx);
+/* Page-locks caller memory so copies from it are asynchronous (IOBuffers). */
+OPE_B200_API int ope_b200_host_register(void* ptr, size_t bytes);
+OPE_B200_API int ope_b200_host_unregister(void* ptr);
+/* Enqueues one buffer (A*B A-scans at h_in); returns a ticket. Fails with
+ * OPE_B200_E_STATE when every slot still holds an unreleased frame. */
+OPE_B200_API int ope_b200_submit(ope_b200_ctx* ctx, const void* h_in, uint64_t* ticket);
+/* Same, with the output copied into the caller's buffer h_out (A*B*(N/2)
+ * floats; page-locked for an asynchronous copy) instead of the slot's own. */
+OPE_B200_API int ope_b200_submit_to(ope_b200_ctx* ctx, const void* h_in, float* h_out, uint64_t* ticket);
+/* Waits until h_in of `ticket` has been copied to the device (the caller may
+ * then reuse it); timeout_ms < 0 waits without limit. */
+OPE_B200_API int ope_b200_input_released(ope_b200_ctx* ctx, uint64_t ticket, int32_t timeout_ms);
+/* Waits for the frame; *h_out points at its A*B*(N/2) floats in pinned host
+ * memory, valid until ope_b200_release(ticket). */
+OPE_B200_API int ope_b200_wait(ope_b200_ctx* ctx, uint64_t ticket, int32_t timeout_ms, const float** h_out);
+OPE_B200_API int ope_b200_release(ope_b200_ctx* ctx, uint64_t ticket);
 
 /* ---- fixed-pattern noise: ProcessingBackend::{request,set,get}FixedPatternNoise*
  *      (backend_interface.h:45-47). Profiles are interleaved (re, im) pairs. ---- */

@@ -6,6 +6,9 @@
 * ``lib/libope_host.so`` -- the C++ host layer (ope::Processor,
   ope::ProcessorConfiguration, ope::IOBuffer, ope::B200Backend) on top of the C
   ABI, for C++ callers of the reference API.
+* ``lib/octproengine<EXT_SUFFIX>`` -- the Python module ``octproengine`` (the
+  reference's Python API) over the host layer; import it with ``lib`` on
+  ``sys.path`` or through ``octproengine_b200.reference_api()``.
 
 Objects are rebuilt only when a source or any header of the package is newer.
 Run ``python -m octproengine_b200.build`` (or ``__graft_entry__.build()``).
@@ -18,11 +21,13 @@ import os
 import shutil
 import subprocess
 import sys
+import sysconfig
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 HOST = os.path.join(PKG, "host")
+PYBIND = os.path.join(PKG, "pybind")
 LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "_build")
 INCLUDE = os.path.join(ROOT, "include")
@@ -41,6 +46,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread", "-I"
 
 CHAIN_LIB = os.path.join(LIBDIR, "libope_b200.so")
 HOST_LIB = os.path.join(LIBDIR, "libope_host.so")
+PY_MODULE = os.path.join(LIBDIR, "octproengine" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
 
 
 def _headers(d: str):
@@ -100,11 +106,29 @@ def build_host(verbose: bool = False) -> str:
     return HOST_LIB
 
 
+def build_python_module(verbose: bool = False) -> str:
+    srcs = sorted(glob.glob(os.path.join(PYBIND, "*.cpp")))
+    if not srcs:
+        return ""
+    try:
+        import pybind11
+    except ImportError as e:  # pragma: no cover - pybind11 ships with the image
+        raise RuntimeError("pybind11 is required to build the octproengine Python module") from e
+    deps = srcs + _headers(HOST) + [HOST_LIB]
+    if _stale(PY_MODULE, deps):
+        cxx = shutil.which("g++") or "g++"
+        _run([cxx] + CXX_FLAGS + ["-fvisibility=hidden", "-shared", "-I", pybind11.get_include(),
+                                  "-I", sysconfig.get_paths()["include"], "-o", PY_MODULE] + srcs +
+             ["-L", LIBDIR, "-lope_host", "-lope_b200", "-Wl,-rpath,$ORIGIN"], verbose)
+    return PY_MODULE
+
+
 def build(verbose: bool = False) -> None:
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
     build_chain(verbose=verbose)
     build_host(verbose=verbose)
+    build_python_module(verbose=verbose)
 
 
 if __name__ == "__main__":

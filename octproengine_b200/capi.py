@@ -94,6 +94,14 @@ SIGNATURES = {
     "ope_b200_process_host": (ctypes.c_int, [_P, _P, _P]),
     "ope_b200_process_bins_device": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "ope_b200_test_inject_copy_stall": (ctypes.c_int, [_P, ctypes.c_uint32]),
+    "ope_b200_ring_depth": (ctypes.c_int, [_P]),
+    "ope_b200_host_register": (ctypes.c_int, [_P, _SZ]),
+    "ope_b200_host_unregister": (ctypes.c_int, [_P]),
+    "ope_b200_submit": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "ope_b200_submit_to": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "ope_b200_input_released": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32]),
+    "ope_b200_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(_FP)]),
+    "ope_b200_release": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "ope_b200_request_fpn_determination": (ctypes.c_int, [_P]),
     "ope_b200_set_fpn_profile": (ctypes.c_int, [_P, _FP, _SZ]),
     "ope_b200_get_fpn_profile": (ctypes.c_int, [_P, _FP, _SZ, ctypes.POINTER(_SZ)]),
@@ -247,6 +255,33 @@ class Context:
         self.check(lib().ope_b200_process_host(self.h, raw.ctypes.data_as(ctypes.c_void_p),
                                                out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+    # streaming ring
+    def submit(self, h_in_ptr: int) -> int:
+        t = ctypes.c_uint64(0)
+        self.check(lib().ope_b200_submit(self.h, h_in_ptr, ctypes.byref(t)))
+        return t.value
+
+    def submit_to(self, h_in_ptr: int, h_out_ptr: int) -> int:
+        """Like submit, but the frame's output is copied into the caller's host
+        buffer h_out_ptr (page-locked for an asynchronous copy)."""
+        t = ctypes.c_uint64(0)
+        self.check(lib().ope_b200_submit_to(self.h, h_in_ptr, h_out_ptr, ctypes.byref(t)))
+        return t.value
+
+    def input_released(self, ticket: int, timeout_ms: int = -1) -> None:
+        self.check(lib().ope_b200_input_released(self.h, ticket, timeout_ms))
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> np.ndarray:
+        """Waits for the frame; returns a zero-copy view of its output (valid until release)."""
+        p = _FP()
+        self.check(lib().ope_b200_wait(self.h, ticket, timeout_ms, ctypes.byref(p)))
+        n = self.cfg.signal_length
+        m = self.cfg.ascans_per_bscan * self.cfg.bscans_per_buffer
+        return np.ctypeslib.as_array(p, shape=(m, n // 2))
+
+    def release(self, ticket: int) -> None:
+        self.check(lib().ope_b200_release(self.h, ticket))
 
     def synchronize(self) -> int:
         st = ctypes.c_int32(0)

@@ -15,8 +15,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ope_b200.h"
@@ -100,6 +102,21 @@ struct ope_b200_ctx {
 
     // test hook: next launch skips its first bulk copy and waits at most this long
     unsigned long long inject_stall_ns = 0;
+
+    // streaming ring (ope_b200_submit / wait / release)
+    struct RingSlot {
+        cudaStream_t stream = nullptr;
+        void* d_in = nullptr;
+        float* d_out = nullptr;
+        float* h_out = nullptr;  // pinned
+        float* h_dst = nullptr;  // where this frame's output lands (h_out or the caller's buffer)
+        cudaEvent_t ev_in = nullptr, ev_done = nullptr;
+        uint64_t ticket = 0;
+        bool busy = false;
+    };
+    std::vector<RingSlot> ring;
+    uint64_t next_ticket = 1;
+    cudaEvent_t ev_last_compute = nullptr;
 
     std::string err;
     std::mutex mu;
@@ -295,12 +312,17 @@ void ope_b200_config_default(ope_b200_config* c) {
     c->dc_split = 1;
 }
 
+// why the calling thread's last ope_b200_create failed (ope_b200_last_error(NULL))
+static thread_local std::string t_create_err;
+
 int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out) {
     if (!out) return OPE_B200_E_INVALID;
     *out = nullptr;
+    t_create_err.clear();
     std::string why;
     int rc = validate_cfg(cfg, &why);
     if (rc != OPE_B200_OK) {
+        t_create_err = why;
         std::fprintf(stderr, "ope_b200_create: %s\n", why.c_str());
         return rc;
     }
@@ -313,6 +335,9 @@ int ope_b200_create(const ope_b200_config* cfg, ope_b200_ctx** out) {
     c->out_bytes = static_cast<size_t>(c->m) * (c->n / 2) * sizeof(float);
     c->device = cfg->device;
     auto bail = [&](int code) {
+        cudaError_t e = cudaGetLastError();
+        t_create_err = std::string("device set-up failed on device ") + std::to_string(c->device) + ": " +
+                       cudaGetErrorString(e);
         ope_b200_destroy(c);
         return code;
     };
@@ -335,6 +360,16 @@ void ope_b200_destroy(ope_b200_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& r : c->ring) {
+        if (r.stream) cudaStreamSynchronize(r.stream);
+        cudaFree(r.d_in);
+        cudaFree(r.d_out);
+        cudaFreeHost(r.h_out);
+        if (r.ev_in) cudaEventDestroy(r.ev_in);
+        if (r.ev_done) cudaEventDestroy(r.ev_done);
+        if (r.stream) cudaStreamDestroy(r.stream);
+    }
+    if (c->ev_last_compute) cudaEventDestroy(c->ev_last_compute);
     for (auto& s : c->slot) free_slot(s);
     cudaFree(c->d_tw);
     cudaFree(c->d_status);
@@ -345,7 +380,10 @@ void ope_b200_destroy(ope_b200_ctx* c) {
     delete c;
 }
 
-const char* ope_b200_last_error(const ope_b200_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* ope_b200_last_error(const ope_b200_ctx* c) {
+    if (c) return c->err.c_str();
+    return t_create_err.empty() ? "null context" : t_create_err.c_str();
+}
 
 int ope_b200_update_config(ope_b200_ctx* c, const ope_b200_config* cfg) {
     if (!c || !cfg) return OPE_B200_E_INVALID;
@@ -551,6 +589,166 @@ cudaError_t launch_chain(int n, int in_kind, int interp, const ChainArgs& a, cud
 }
 
 }  // namespace ope_b200
+
+// ---------------------------------------------------------------------------
+// Streaming ring: the IOBuffer path of ProcessingBackend::process
+// (backend_interface.h:24,35-37). Each of num_input_buffers slots owns a
+// stream, device input/output buffers and a pinned host output buffer. A frame
+// is H2D -> chain -> D2H on its slot's stream; the chain of frame i+1 waits for
+// the chain of frame i (FPN state is shared and ordered), so copies of
+// neighbouring frames overlap the computation in both directions.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+bool wait_event_bounded(cudaEvent_t ev, int timeout_ms, cudaError_t* err) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    while (true) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return true;
+        if (e != cudaErrorNotReady) {
+            *err = e;
+            return false;
+        }
+        if (timeout_ms >= 0 &&
+            std::chrono::duration_cast<std::chrono::milliseconds>(clk::now() - t0).count() > timeout_ms) {
+            *err = cudaErrorNotReady;
+            return false;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+int ensure_ring(ope_b200_ctx* c) {
+    if (!c->ring.empty()) return OPE_B200_OK;
+    const int depth = c->cfg.num_input_buffers >= 2 ? c->cfg.num_input_buffers : 2;
+    c->ring.resize(depth);
+    for (auto& r : c->ring) {
+        OPE_CU(c, cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking));
+        OPE_CU(c, cudaMalloc(&r.d_in, c->in_bytes));
+        OPE_CU(c, cudaMalloc(&r.d_out, c->out_bytes));
+        OPE_CU(c, cudaHostAlloc(reinterpret_cast<void**>(&r.h_out), c->out_bytes, cudaHostAllocPortable));
+        OPE_CU(c, cudaEventCreateWithFlags(&r.ev_in, cudaEventDisableTiming));
+        OPE_CU(c, cudaEventCreateWithFlags(&r.ev_done, cudaEventDisableTiming));
+    }
+    OPE_CU(c, cudaEventCreateWithFlags(&c->ev_last_compute, cudaEventDisableTiming));
+    return OPE_B200_OK;
+}
+
+ope_b200_ctx::RingSlot* find_slot(ope_b200_ctx* c, uint64_t ticket) {
+    if (c->ring.empty() || ticket == 0) return nullptr;
+    auto& r = c->ring[(ticket - 1) % c->ring.size()];
+    return (r.busy && r.ticket == ticket) ? &r : nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ope_b200_ring_depth(ope_b200_ctx* c) {
+    if (!c) return OPE_B200_E_INVALID;
+    return c->cfg.num_input_buffers >= 2 ? c->cfg.num_input_buffers : 2;
+}
+
+int ope_b200_host_register(void* ptr, size_t bytes) {
+    if (!ptr || !bytes) return OPE_B200_E_INVALID;
+    return cudaHostRegister(ptr, bytes, cudaHostRegisterPortable) == cudaSuccess ? OPE_B200_OK : OPE_B200_E_CUDA;
+}
+
+int ope_b200_host_unregister(void* ptr) {
+    if (!ptr) return OPE_B200_E_INVALID;
+    return cudaHostUnregister(ptr) == cudaSuccess ? OPE_B200_OK : OPE_B200_E_CUDA;
+}
+
+int ope_b200_submit(ope_b200_ctx* c, const void* h_in, uint64_t* ticket) {
+    return ope_b200_submit_to(c, h_in, nullptr, ticket);
+}
+
+int ope_b200_submit_to(ope_b200_ctx* c, const void* h_in, float* h_out_dst, uint64_t* ticket) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!h_in || !ticket) return fail(c, OPE_B200_E_INVALID, "null input buffer or ticket");
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    int rc = ensure_ring(c);
+    if (rc != OPE_B200_OK) return rc;
+    const uint64_t t = c->next_ticket;
+    auto& r = c->ring[(t - 1) % c->ring.size()];
+    if (r.busy)
+        return fail(c, OPE_B200_E_STATE,
+                    "all ring slots are in use: release the oldest frame's output before submitting more");
+    OPE_CU(c, cudaMemcpyAsync(r.d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, r.stream));
+    OPE_CU(c, cudaEventRecord(r.ev_in, r.stream));
+    OPE_CU(c, cudaStreamWaitEvent(r.stream, c->ev_last_compute, 0));
+    rc = process_locked(c, r.d_in, r.d_out, c->m, r.stream);
+    if (rc != OPE_B200_OK) return rc;
+    OPE_CU(c, cudaEventRecord(c->ev_last_compute, r.stream));
+    r.h_dst = h_out_dst ? h_out_dst : r.h_out;
+    OPE_CU(c, cudaMemcpyAsync(r.h_dst, r.d_out, c->out_bytes, cudaMemcpyDeviceToHost, r.stream));
+    OPE_CU(c, cudaEventRecord(r.ev_done, r.stream));
+    r.busy = true;
+    r.ticket = t;
+    c->next_ticket++;
+    *ticket = t;
+    return OPE_B200_OK;
+}
+
+int ope_b200_input_released(ope_b200_ctx* c, uint64_t ticket, int32_t timeout_ms) {
+    if (!c) return OPE_B200_E_INVALID;
+    cudaEvent_t ev;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        auto* r = find_slot(c, ticket);
+        if (!r) return fail(c, OPE_B200_E_INVALID, "unknown or released ticket");
+        ev = r->ev_in;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!wait_event_bounded(ev, timeout_ms, &e))
+        return e == cudaErrorNotReady ? OPE_B200_E_TIMEOUT : OPE_B200_E_CUDA;
+    return OPE_B200_OK;
+}
+
+int ope_b200_wait(ope_b200_ctx* c, uint64_t ticket, int32_t timeout_ms, const float** h_out) {
+    if (!c) return OPE_B200_E_INVALID;
+    cudaEvent_t ev;
+    const float* out;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        auto* r = find_slot(c, ticket);
+        if (!r) return fail(c, OPE_B200_E_INVALID, "unknown or released ticket");
+        ev = r->ev_done;
+        out = r->h_dst;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!wait_event_bounded(ev, timeout_ms, &e)) {
+        if (e == cudaErrorNotReady) return OPE_B200_E_TIMEOUT;
+        std::lock_guard<std::mutex> lk(c->mu);
+        return cuda_fail(c, e, "frame");
+    }
+    int st = 0;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        OPE_CU(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st != 0) {
+            cudaMemset(c->d_status, 0, sizeof(int));
+            return fail(c, OPE_B200_E_DEVICE, "kernel reported status " + std::to_string(st));
+        }
+    }
+    if (h_out) *h_out = out;
+    return OPE_B200_OK;
+}
+
+int ope_b200_release(ope_b200_ctx* c, uint64_t ticket) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto* r = find_slot(c, ticket);
+    if (!r) return fail(c, OPE_B200_E_INVALID, "unknown or released ticket");
+    if (cudaEventQuery(r->ev_done) != cudaSuccess) return fail(c, OPE_B200_E_STATE, "frame still in flight");
+    r->busy = false;
+    return OPE_B200_OK;
+}
+
+}  // extern "C"
 
 // ---------------------------------------------------------------------------
 // Fixed-pattern-noise determination without device allocation.
