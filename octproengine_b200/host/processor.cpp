@@ -87,18 +87,23 @@ public:
         return cs;
     }
 
+    // A dimension change since the last initialize() is applied by the
+    // re-initialization at the next buffer request or process(); until then
+    // the backend still holds the old dimensions and gets no updates.
+    bool live() const { return initialized && !dimsChanged(config.dataParams, lastInit); }
+
     void pushResampling() {
-        if (!initialized) return;
+        if (!live()) return;
         auto c = resamplingCurve();
         backend->updateResamplingCurve(c.data(), c.size());
     }
     void pushWindow() {
-        if (!initialized) return;
+        if (!live()) return;
         auto c = windowCurve();
         backend->updateWindowCurve(c.data(), c.size());
     }
     void pushDispersion() {
-        if (!initialized) return;
+        if (!live()) return;
         auto c = dispersionCurve();
         backend->updateDispersionCurve(c.data(), c.size());
     }
@@ -108,7 +113,7 @@ public:
         pushDispersion();
     }
     void pushConfig() {
-        if (initialized) backend->updateConfig(config);
+        if (live()) backend->updateConfig(config);
     }
 
     void pushProfiles() {
@@ -135,9 +140,9 @@ public:
         backend->initialize(config);
         backend->setOutputCallback([this](const IOBuffer& out) { callbacks.invokeAll(out); });
         initialized = true;
+        lastInit = config.dataParams;
         pushCurves();
         pushProfiles();
-        lastInit = config.dataParams;
     }
 
     void ensureInitialized() {

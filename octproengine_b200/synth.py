@@ -46,11 +46,31 @@ class SynthParams:
     noise_sigma: float = 30.0
     dc: float = 32768.0
     background_ripple: bool = False
+    # When set, the wavenumber map is defined by its resampling curve instead of
+    # k_coeffs: raw sample n carries wavenumber index k(n) = r^-1(n) with
+    # r(t) = sum_m c_m t^m, t = j/(n-1) (the reference's resampling polynomial),
+    # so resampling with exactly these coefficients linearises the spectrum.
+    resampling_truth: Optional[tuple] = None
 
 
 def k_map(n: int, coeffs=K_COEFFS) -> np.ndarray:
     x = np.arange(n, dtype=np.float64)
     return coeffs[0] + coeffs[1] * x + coeffs[2] * x ** 2 + coeffs[3] * x ** 3
+
+
+def k_map_from_resampling(n: int, coeffs) -> np.ndarray:
+    """Wavenumber index of each raw sample for a monotone resampling polynomial.
+
+    r(j) = sum_m c_m (j/(n-1))^m gives the raw position at which wavenumber j
+    is sampled; its inverse, evaluated on a 16x oversampled grid and linearly
+    interpolated, gives k(n).
+    """
+    j = np.linspace(0.0, n - 1.0, 16 * (n - 1) + 1)
+    t = j / (n - 1)
+    r = sum(float(coeffs[m]) * t ** m for m in range(4))
+    if np.any(np.diff(r) <= 0):
+        raise ValueError("resampling polynomial is not monotone on [0, n-1]")
+    return np.interp(np.arange(n, dtype=np.float64), r, j)
 
 
 def linearising_coeffs(n: int, coeffs=K_COEFFS) -> tuple:
@@ -81,7 +101,8 @@ def generate(p: SynthParams, device="cpu") -> torch.Tensor:
     n, A, B = p.n, p.ascans, p.bscans
     M = A * B
     dev = torch.device(device)
-    k = torch.tensor(k_map(n, p.k_coeffs), dtype=torch.float64, device=dev)
+    kn = k_map(n, p.k_coeffs) if p.resampling_truth is None else k_map_from_resampling(n, p.resampling_truth)
+    k = torch.tensor(kn, dtype=torch.float64, device=dev)
     kt = k / (n - 1)
     env = torch.exp(-0.5 * ((kt - 0.5) / 0.25) ** 2)
     psi = p.d2 * (kt - 0.5) ** 2 + p.d3 * (kt - 0.5) ** 3
