@@ -201,6 +201,44 @@ OPE_B200_API int ope_b200_generate_window_curve(int32_t n, int32_t window_type, 
                                                 float* out);
 OPE_B200_API int ope_b200_phase_to_cos_sin(const float* phase, size_t n, float* out_interleaved);
 
+/* ---- differentiable chain for autofocus. No counterpart in the reference (its
+ *      dispersion and k-mapping coefficients are set by hand or swept,
+ *      processor.cpp:371-470); the forward follows the chain of
+ *      CpuBackend::Impl::processData (cpu_backend.cpp:184-264). ----
+ *
+ * Parameters live in DEVICE memory as float[8]: the dispersion polynomial
+ * d0..d3 and the resampling polynomial c0..c3, both in the convention of
+ * ProcessorConfiguration::generate{Dispersion,Resampling}Curve
+ * (processorconfiguration.cpp:438-482). Every call rebuilds the resampling and
+ * window-phase tables on the device from them, so a parameter update needs no
+ * host round trip. Each A-scan's integer mean is subtracted before the chain
+ * and not added back (the image without its DC term). One handle serves one
+ * stream at a time: its tables and partial sums are shared by its calls. */
+typedef struct ope_b200_af ope_b200_af;
+#define OPE_B200_AF_OUT_INTENSITY 1 /* I = |X|^2, bins [0, N/2)            */
+#define OPE_B200_AF_OUT_DB 2        /* 10 log10(I / (N/2)), the reference's log
+                                       scale before the grayscale affine map   */
+/* n in {1024, 2048, 4096}; input_dtype an ope::DataType (UINT8, UINT16, FLOAT32
+ * -- read as float); interpolation an ope::InterpolationMethod; window: N host
+ * floats (NULL = rectangular), copied. */
+OPE_B200_API int ope_b200_af_create(int32_t n, int32_t input_dtype, int32_t interpolation, const float* window,
+                                    int32_t device, ope_b200_af** out);
+OPE_B200_API void ope_b200_af_destroy(ope_b200_af* af);
+OPE_B200_API const char* ope_b200_af_last_error(const ope_b200_af* af);
+/* Forward over num_ascans A-scans at d_in (16-byte aligned). d_out (may be
+ * NULL): num_ascans x N/2 floats in `output_mode`. d_hs (may be NULL): two
+ * doubles, the Shannon entropy H = -sum p ln p of the normalised intensity
+ * p = I / S over every bin of every A-scan, and S = sum I. */
+OPE_B200_API int ope_b200_af_forward(ope_b200_af* af, const void* d_in, int64_t num_ascans, const float* d_params,
+                                     int32_t output_mode, float* d_out, double* d_hs, void* stream);
+/* Adjoint: writes dL/dparams (float[8], device) for L = sum(d_grad_out * out)
+ * when d_grad_out (num_ascans x N/2, gradient of the `output_mode` output) is
+ * given, else for L = H using d_hs from ope_b200_af_forward with the same
+ * parameters. Recomputes the forward (nothing is stored between the calls). */
+OPE_B200_API int ope_b200_af_backward(ope_b200_af* af, const void* d_in, int64_t num_ascans, const float* d_params,
+                                      int32_t output_mode, const float* d_grad_out, const double* d_hs,
+                                      float* d_grad_params, void* stream);
+
 /* Test hook, no reference counterpart: the next launch of this context skips
  * its first input copy, so its bounded wait runs out after `timeout_us`; the
  * kernel then records a status that ope_b200_synchronize / process_host

@@ -1,0 +1,354 @@
+"""Differentiable OCT chain and gradient autofocus on B200.
+
+The reference sets dispersion and k-linearisation coefficients by hand
+(Processor::setDispersionCoefficients / setResamplingCoefficients,
+src/core/processor.cpp:371-470); the usual way to find them is a parameter
+sweep of the whole chain. Here the chain is differentiable: the hand-written
+adjoint kernels behind ``ope_b200_af_backward`` (octproengine_b200/csrc/
+autofocus.cuh) give the gradient of an image objective with respect to the
+8 chain parameters
+
+    params = (d0, d1, d2, d3, c0, c1, c2, c3)
+
+-- the dispersion polynomial and the resampling polynomial in the reference's
+convention (processorconfiguration.cpp:438-482, t = j/(N-1)) -- so autofocus
+becomes a gradient fit.
+
+* :class:`Autofocus` -- one ``ope_b200_af`` handle (signal length, input type,
+  interpolation, window) with raw forward / adjoint calls on device tensors;
+* :class:`ChainImage` and :class:`ChainEntropy` -- ``torch.autograd.Function``
+  wrappers: the image (intensity or dB) or the Shannon entropy of the
+  normalised intensity, differentiable with respect to ``params``;
+* :func:`fit_dispersion` -- BFGS on (d2, d3) of the centred dispersion phase
+  psi(t) = d2 (t-1/2)^2 + d3 (t-1/2)^3, entropy objective;
+* :func:`grid_sweep` -- the parameter sweep it replaces, every grid point one
+  launch of the same forward chain, all enqueued back to back.
+
+Everything runs on the GPU through the C ABI; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import capi
+
+OUT_INTENSITY = 1
+OUT_DB = 2
+LINEAR, CUBIC, LANCZOS = 0, 1, 2  # ope::InterpolationMethod
+
+_DTYPES = {"uint8": 1, "uint16": 2, "float32": 9}  # ope::DataType
+_TORCH_DTYPES = {"uint8": torch.uint8, "uint16": torch.int16, "float32": torch.float32}
+
+# psi(t) = d2 (t-1/2)^2 + d3 (t-1/2)^3 expanded in powers of t: d = M @ (d2, d3)
+CENTRED_TO_POLY = np.array([[0.25, -0.125], [-1.0, 0.75], [1.0, -1.5], [0.0, 1.0]])
+
+
+def dispersion_poly(d2: float, d3: float) -> np.ndarray:
+    """Reference-convention dispersion coefficients of the centred (d2, d3)."""
+    return CENTRED_TO_POLY @ np.array([d2, d3], dtype=np.float64)
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream) -> ctypes.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Autofocus:
+    """The differentiable chain for one geometry: N samples per A-scan, one
+    input type, one interpolation, one window. One handle serves one stream
+    at a time (its device tables and partial sums are shared by its calls)."""
+
+    def __init__(self, n: int, input_dtype: str = "uint16", interpolation: int = LANCZOS,
+                 window: Optional[np.ndarray] = None, device: int = 0):
+        if input_dtype not in _DTYPES:
+            raise ValueError(f"input_dtype must be one of {sorted(_DTYPES)}")
+        self.n = int(n)
+        self.input_dtype = input_dtype
+        self.interpolation = int(interpolation)
+        self.device = torch.device("cuda", device)
+        h = ctypes.c_void_p()
+        w = None
+        if window is not None:
+            self._window = np.ascontiguousarray(window, np.float32)
+            if self._window.size != self.n:
+                raise ValueError("window must have N values")
+            w = capi.fptr(self._window)
+        rc = capi.lib().ope_b200_af_create(self.n, _DTYPES[input_dtype], self.interpolation, w, device,
+                                           ctypes.byref(h))
+        if rc != capi.OK:
+            raise capi.B200Error(rc, f"autofocus handle for N={n}, {input_dtype}, interpolation {interpolation}")
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            capi.lib().ope_b200_af_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != capi.OK:
+            raise capi.B200Error(rc, capi.lib().ope_b200_af_last_error(self.h).decode())
+
+    def _check_raw(self, raw: torch.Tensor) -> int:
+        if raw.device.type != "cuda" or raw.dtype != _TORCH_DTYPES[self.input_dtype]:
+            raise TypeError(f"raw must be a CUDA tensor of {_TORCH_DTYPES[self.input_dtype]}")
+        if raw.dim() != 2 or raw.shape[1] != self.n or not raw.is_contiguous():
+            raise ValueError(f"raw must be a contiguous (A-scans, {self.n}) tensor")
+        return raw.shape[0]
+
+    @staticmethod
+    def _check_params(params: torch.Tensor) -> None:
+        if params.device.type != "cuda" or params.dtype != torch.float32 or params.numel() != 8:
+            raise TypeError("params must be a CUDA float32 tensor of 8 values (d0..d3, c0..c3)")
+
+    def forward(self, raw: torch.Tensor, params: torch.Tensor, output: int = OUT_INTENSITY,
+                out: Optional[torch.Tensor] = None, hs: Optional[torch.Tensor] = None, stream=None) -> None:
+        """Image (``out``, A-scans x N/2 float32) and/or (H, S) (``hs``, 2 float64)."""
+        m = self._check_raw(raw)
+        self._check_params(params)
+        self._check(capi.lib().ope_b200_af_forward(self.h, _ptr(raw), m, _ptr(params), output, _ptr(out), _ptr(hs),
+                                                   _stream(stream)))
+
+    def backward(self, raw: torch.Tensor, params: torch.Tensor, grad: torch.Tensor,
+                 grad_out: Optional[torch.Tensor] = None, hs: Optional[torch.Tensor] = None,
+                 output: int = OUT_INTENSITY, stream=None) -> None:
+        """dL/dparams into ``grad`` (8 float32): L = sum(grad_out * image) or L = H."""
+        m = self._check_raw(raw)
+        self._check_params(params)
+        if grad_out is not None and (grad_out.dtype != torch.float32 or not grad_out.is_contiguous()
+                                     or grad_out.shape != (m, self.n // 2)):
+            raise ValueError("grad_out must be a contiguous float32 (A-scans, N/2) tensor")
+        self._check(capi.lib().ope_b200_af_backward(self.h, _ptr(raw), m, _ptr(params), output, _ptr(grad_out),
+                                                    _ptr(hs), _ptr(grad), _stream(stream)))
+
+
+class ChainImage(torch.autograd.Function):
+    """image = chain(raw; params): intensity |X|^2 or 10 log10(|X|^2/(N/2))."""
+
+    @staticmethod
+    def forward(ctx, raw, params, af: Autofocus, output: int = OUT_INTENSITY):
+        p = params.detach().contiguous()
+        out = torch.empty((raw.shape[0], af.n // 2), dtype=torch.float32, device=raw.device)
+        af.forward(raw, p, output=output, out=out)
+        ctx.save_for_backward(raw, p)
+        ctx.af, ctx.output = af, output
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        raw, p = ctx.saved_tensors
+        grad = torch.empty(8, dtype=torch.float32, device=raw.device)
+        ctx.af.backward(raw, p, grad, grad_out=g.contiguous().float(), output=ctx.output)
+        return None, grad, None, None
+
+
+class ChainEntropy(torch.autograd.Function):
+    """H(params) = -sum p ln p, p = I / sum I over every bin of every A-scan."""
+
+    @staticmethod
+    def forward(ctx, raw, params, af: Autofocus):
+        p = params.detach().contiguous()
+        hs = torch.empty(2, dtype=torch.float64, device=raw.device)
+        af.forward(raw, p, hs=hs)
+        ctx.save_for_backward(raw, p, hs)
+        ctx.af = af
+        return hs[0].clone()
+
+    @staticmethod
+    def backward(ctx, g):
+        raw, p, hs = ctx.saved_tensors
+        grad = torch.empty(8, dtype=torch.float32, device=raw.device)
+        ctx.af.backward(raw, p, grad, hs=hs)
+        return None, grad * g.to(torch.float32), None
+
+
+@dataclass
+class FitResult:
+    d2: float
+    d3: float
+    entropy: float
+    iterations: int
+    evaluations: int
+    seconds: float
+    history: list = field(default_factory=list)  # (d2, d3, H, seconds since start) per iteration
+
+
+class _Evaluator:
+    """H and dH/d(d2, d3) at a point, one host round trip per evaluation.
+
+    With ``graph`` the whole evaluation (parameter upload from pinned host
+    memory, forward, adjoint, result download) is captured once in a CUDA
+    graph and replayed, so an evaluation costs one graph launch and one
+    synchronisation on the host.
+    """
+
+    def __init__(self, af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], graph: bool = True):
+        self.af, self.raw = af, raw
+        dev = raw.device
+        self.kmap = np.asarray(kmap, np.float32)
+        self.h_params = torch.empty(8, dtype=torch.float32, pin_memory=True)
+        self.d_params = torch.empty(8, dtype=torch.float32, device=dev)
+        self.d_hs = torch.empty(2, dtype=torch.float64, device=dev)
+        self.d_grad = torch.empty(8, dtype=torch.float32, device=dev)
+        self.h_hs = torch.empty(2, dtype=torch.float64, pin_memory=True)
+        self.h_grad = torch.empty(8, dtype=torch.float32, pin_memory=True)
+        self.count = 0
+        self.graph = None
+        self._set(np.zeros(2))
+        if graph:
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(torch.cuda.current_stream(dev))
+            with torch.cuda.stream(side):
+                self._enqueue(side)  # warm-up outside the capture
+            side.synchronize()
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph, stream=side):
+                self._enqueue(side)
+        self.stream = torch.cuda.current_stream(dev)
+
+    def _set(self, theta) -> None:
+        hp = self.h_params.numpy()
+        hp[:4] = dispersion_poly(theta[0], theta[1])
+        hp[4:] = self.kmap
+
+    def _enqueue(self, stream) -> None:
+        self.d_params.copy_(self.h_params, non_blocking=True)
+        self.af.forward(self.raw, self.d_params, hs=self.d_hs, stream=stream)
+        self.af.backward(self.raw, self.d_params, self.d_grad, hs=self.d_hs, stream=stream)
+        self.h_hs.copy_(self.d_hs, non_blocking=True)
+        self.h_grad.copy_(self.d_grad, non_blocking=True)
+
+    def __call__(self, theta: np.ndarray):
+        self._set(theta)
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._enqueue(self.stream)
+        torch.cuda.current_stream(self.raw.device).synchronize()
+        self.count += 1
+        g = CENTRED_TO_POLY.T @ self.h_grad.numpy()[:4].astype(np.float64)
+        return float(self.h_hs[0]), g
+
+
+def fit_dispersion(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], init=(0.0, 0.0),
+                   max_iter: int = 60, step_tol: float = 1e-3, first_step: float = 2.0,
+                   graph: bool = True) -> FitResult:
+    """Minimises the image entropy over the centred dispersion (d2, d3).
+
+    BFGS with an Armijo backtracking line search on the host (2 x 2 inverse
+    Hessian); each evaluation is one forward (entropy) and one adjoint pass on
+    the device, replayed from a CUDA graph when ``graph`` is set (the capture
+    happens before the clock starts). ``kmap`` holds the resampling
+    coefficients c0..c3. Stops when a step moves less than ``step_tol`` (rad).
+    """
+    ev = _Evaluator(af, raw, kmap, graph=graph)
+    t0 = time.perf_counter()
+    x = np.asarray(init, np.float64)
+    f, g = ev(x)
+    gmax = float(np.abs(g).max())
+    hinv = np.eye(2) * (first_step / gmax if gmax > 0 else 1.0)
+    hist = [(float(x[0]), float(x[1]), f, time.perf_counter() - t0)]
+    it = 0
+    for it in range(1, max_iter + 1):
+        d = -hinv @ g
+        if g @ d >= 0:  # not a descent direction: restart from steepest descent
+            hinv = np.eye(2) * (first_step / max(float(np.abs(g).max()), 1e-30))
+            d = -hinv @ g
+        step = 1.0
+        while True:
+            xn = x + step * d
+            fn, gn = ev(xn)
+            if fn <= f + 1e-4 * step * float(g @ d) or step < 1e-6:
+                break
+            step *= 0.5
+        s, yv = xn - x, gn - g
+        sy = float(s @ yv)
+        if sy > 1e-30:
+            rho = 1.0 / sy
+            eye = np.eye(2)
+            hinv = (eye - rho * np.outer(s, yv)) @ hinv @ (eye - rho * np.outer(yv, s)) + rho * np.outer(s, s)
+        x, f, g = xn, fn, gn
+        hist.append((float(x[0]), float(x[1]), f, time.perf_counter() - t0))
+        if float(np.linalg.norm(s)) < step_tol:
+            break
+    secs = time.perf_counter() - t0
+    return FitResult(float(x[0]), float(x[1]), f, it, ev.count, secs, hist)
+
+
+@dataclass
+class SweepResult:
+    d2: float
+    d3: float
+    entropy: float
+    seconds: float
+    grid: np.ndarray  # (n2, n3) entropies
+    capture_seconds: float = 0.0
+
+
+def grid_sweep(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], d2_range=(-40.0, 40.0),
+               d3_range=(-20.0, 20.0), n2: int = 64, n3: int = 64, graph: bool = True) -> SweepResult:
+    """Entropy of the forward chain at every point of an n2 x n3 (d2, d3) grid.
+
+    All parameter vectors are uploaded once; the n2*n3 forward passes run back
+    to back on one stream -- replayed from one CUDA graph when ``graph`` is set
+    (captured before the clock starts, its capture time reported apart) --
+    with one synchronisation at the end.
+    """
+    dev = raw.device
+    g2 = np.linspace(d2_range[0], d2_range[1], n2)
+    g3 = np.linspace(d3_range[0], d3_range[1], n3)
+    P = np.empty((n2 * n3, 8), np.float32)
+    k = 0
+    for a in g2:
+        for b in g3:
+            P[k, :4] = dispersion_poly(a, b)
+            P[k, 4:] = kmap
+            k += 1
+    d_params = torch.from_numpy(P).to(dev)
+    hs = torch.empty((n2 * n3, 2), dtype=torch.float64, device=dev)
+
+    def enqueue(stream):
+        for k in range(n2 * n3):
+            af.forward(raw, d_params[k], hs=hs[k], stream=stream)
+
+    g = None
+    cap = 0.0
+    if graph:
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            af.forward(raw, d_params[0], hs=hs[0], stream=side)  # warm-up outside the capture
+        side.synchronize()
+        t_c = time.perf_counter()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            enqueue(side)
+        torch.cuda.synchronize(dev)
+        cap = time.perf_counter() - t_c
+    stream = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    if g is not None:
+        g.replay()
+    else:
+        enqueue(stream)
+    best = int(torch.argmin(hs[:, 0]).item())  # synchronises
+    secs = time.perf_counter() - t0
+    H = hs[:, 0].cpu().numpy().reshape(n2, n3)
+    return SweepResult(float(g2[best // n3]), float(g3[best % n3]), float(H.flat[best]), secs, H, cap)

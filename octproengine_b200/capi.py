@@ -115,6 +115,12 @@ SIGNATURES = {
     "ope_b200_generate_window_curve": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                                       ctypes.c_float, _FP]),
     "ope_b200_phase_to_cos_sin": (ctypes.c_int, [_FP, _SZ, _FP]),
+    "ope_b200_af_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _FP, ctypes.c_int32,
+                                           ctypes.POINTER(_P)]),
+    "ope_b200_af_destroy": (None, [_P]),
+    "ope_b200_af_last_error": (ctypes.c_char_p, [_P]),
+    "ope_b200_af_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P]),
+    "ope_b200_af_backward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P, _P]),
     "ope_b200_abi_version": (ctypes.c_int, []),
     "ope_b200_device_supported": (ctypes.c_int, [ctypes.c_int32]),
 }

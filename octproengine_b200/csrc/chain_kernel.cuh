@@ -518,12 +518,14 @@ OPE_HD void fft_load(int t, const float4* exch, cp* v) {
     }
 }
 
-template <int N, int P>
+// FULL = true computes every output of the last pass (all N bins); by default
+// the last pass keeps only bins [0, N/2).
+template <int N, int P, bool FULL = false>
 OPE_HD void fft_twiddle_dft(int t, cp* v, const float2* tw) {
     using PI = PassInfo<N, P>;
     constexpr int T = Plan<N>::T;
     constexpr int R = PI::R, D = PI::D, NS = PI::NS;
-    constexpr int NOUT = PI::LAST ? R / 2 : R;
+    constexpr int NOUT = (PI::LAST && !FULL) ? R / 2 : R;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
         cp u[R];

@@ -1,0 +1,213 @@
+"""Differentiable chain (autofocus): forward, hand-written adjoint, fit.
+
+CPU tests check the float64 oracle itself (its autograd against central
+finite differences) and the host-side parameter maps. GPU tests call the C ABI
+(ope_b200_af_forward / ope_b200_af_backward) through
+octproengine_b200.autofocus and compare with the float64 oracle:
+forward image and entropy, adjoint gradients for all 8 parameters (entropy
+objective and arbitrary image gradients, intensity and dB outputs), central
+finite differences of the GPU forward, and the BFGS fit against hidden
+dispersion coefficients.
+"""
+import numpy as np
+import pytest
+import torch
+
+from octproengine_b200 import synth
+from oracle import autofocus64 as O
+from oracle import restate as R
+
+N = 2048
+
+
+def make_case(m=64, seed=5, d2=12.0, d3=-7.0, kpert=1.1, dtype="uint16"):
+    kc = list(synth.K_COEFFS)
+    kc[3] *= kpert
+    ctrue = synth.linearising_coeffs(N, tuple(kc))
+    p = synth.SynthParams(n=N, ascans=m, seed=seed, d2=d2, d3=d3, resampling_truth=ctrue, dtype=dtype)
+    raw_t = synth.generate(p)
+    raw = synth.as_numpy(raw_t, dtype)
+    window = R.window_curve(N, R.HANN, 0.5, 0.95)
+    return raw_t, raw, window, ctrue
+
+
+def params_of(d2, d3, kmap):
+    from octproengine_b200.autofocus import dispersion_poly
+    return np.concatenate([dispersion_poly(d2, d3), np.asarray(kmap, np.float64)]).astype(np.float32)
+
+
+# ------------------------------------------------------------------ CPU --
+
+def test_centred_map_matches_generator_convention():
+    from octproengine_b200.autofocus import dispersion_poly
+    for d2, d3 in [(1.0, 0.0), (0.0, 1.0), (-13.5, 7.25)]:
+        assert np.allclose(dispersion_poly(d2, d3), synth.compensating_coeffs(d2, d3))
+
+
+@pytest.mark.parametrize("interp", [O.LINEAR, O.CUBIC, O.LANCZOS])
+def test_oracle_gradient_matches_finite_differences(interp):
+    _, raw, window, ctrue = make_case(m=8)
+    p0 = params_of(9.0, -4.0, ctrue).astype(np.float64)
+    H0, g = O.entropy_and_grad(raw, p0, window, interp, f32_curves=False)
+    # linear interpolation is only piecewise differentiable in the positions:
+    # a small step keeps the difference quotient off the kinks at integer r
+    h = 1e-6 if interp == O.LINEAR else 1e-3
+    for k in range(8):
+        e = np.zeros(8)
+        e[k] = h
+        fd = (O.entropy_and_grad(raw, p0 + e, window, interp, f32_curves=False)[0] -
+              O.entropy_and_grad(raw, p0 - e, window, interp, f32_curves=False)[0]) / (2 * h)
+        assert abs(fd - g[k]) <= 2e-3 * np.abs(g).max() + 1e-3 * abs(g[k]), (k, fd, g[k])
+
+
+def test_polynomial_wavenumber_map_inverts_resampling():
+    c = synth.linearising_coeffs(N)
+    k = synth.k_map_from_resampling(N, c)
+    j = np.arange(N) / (N - 1.0)
+    r = sum(c[m] * j ** m for m in range(4))
+    inside = (r >= 0) & (r <= N - 1)  # wavenumbers sampled inside the raw record
+    assert inside.sum() > N - 8
+    err = np.interp(r, np.arange(N), k) - np.arange(N)
+    assert np.max(np.abs(err[inside])) < 1e-3
+
+
+# ------------------------------------------------------------------ GPU --
+
+def _af(cuda, interp, window, dtype="uint16"):
+    from octproengine_b200.autofocus import Autofocus
+    return Autofocus(N, dtype, interp, window=window)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("interp", [O.LINEAR, O.CUBIC, O.LANCZOS])
+def test_forward_matches_fp64(cuda, interp):
+    from octproengine_b200.autofocus import OUT_INTENSITY, OUT_DB
+    raw_t, raw, window, ctrue = make_case(m=64)
+    p = params_of(10.0, -5.0, ctrue)
+    af = _af(cuda, interp, window)
+    d_raw = raw_t.to(cuda)
+    d_p = torch.from_numpy(p).to(cuda)
+    I = torch.empty((64, N // 2), dtype=torch.float32, device=cuda)
+    dB = torch.empty_like(I)
+    hs = torch.empty(2, dtype=torch.float64, device=cuda)
+    af.forward(d_raw, d_p, OUT_INTENSITY, out=I, hs=hs)
+    af.forward(d_raw, d_p, OUT_DB, out=dB)
+    torch.cuda.synchronize()
+    I64, _ = O.intensity(raw, p.astype(np.float64), window, interp)
+    I64 = I64.numpy()
+    shown = I64 > I64.max() * 1e-5  # within 50 dB of the strongest bin
+    err_db = np.abs(10 * np.log10(I.cpu().numpy()[shown].astype(np.float64) / I64[shown]))
+    assert err_db.max() < 0.02, err_db.max()
+    ref_db = 10 * np.log10(I64 / (N // 2))
+    assert np.abs(dB.cpu().numpy()[shown] - ref_db[shown]).max() < 0.02
+    H64 = float(O.entropy_of(torch.as_tensor(I64)))
+    assert abs(hs[0].item() - H64) < 1e-6 * H64
+    assert abs(hs[1].item() - I64.sum()) < 1e-5 * I64.sum()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("interp", [O.LINEAR, O.CUBIC, O.LANCZOS])
+def test_entropy_gradient_matches_fp64(cuda, interp):
+    from octproengine_b200.autofocus import ChainEntropy
+    raw_t, raw, window, ctrue = make_case(m=64, seed=7)
+    p = params_of(4.0, 3.0, np.asarray(ctrue) + np.array([0.0, 0.0, 1.5, -1.0]))
+    af = _af(cuda, interp, window)
+    d_p = torch.from_numpy(p).to(cuda).requires_grad_(True)
+    H = ChainEntropy.apply(raw_t.to(cuda), d_p, af)
+    H.backward()
+    g = d_p.grad.cpu().numpy().astype(np.float64)
+    H64, g64 = O.entropy_and_grad(raw, p.astype(np.float64), window, interp)
+    assert abs(H.item() - H64) < 1e-6 * H64
+    scale = np.abs(g64).max()
+    assert np.all(np.abs(g - g64) <= 1e-2 * scale + 1e-2 * np.abs(g64)), (g, g64)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("db", [False, True])
+def test_image_gradient_matches_fp64(cuda, db):
+    from octproengine_b200.autofocus import ChainImage, OUT_DB, OUT_INTENSITY
+    raw_t, raw, window, ctrue = make_case(m=32, seed=9)
+    p = params_of(-6.0, 2.0, ctrue)
+    af = _af(cuda, O.LANCZOS, window)
+    rng = np.random.default_rng(3)
+    G = rng.standard_normal((32, N // 2)).astype(np.float32)
+    if not db:
+        G *= 1e-12  # intensities are ~1e12: keep the objective O(1)
+    d_p = torch.from_numpy(p).to(cuda).requires_grad_(True)
+    img = ChainImage.apply(raw_t.to(cuda), d_p, af, OUT_DB if db else OUT_INTENSITY)
+    (img * torch.from_numpy(G).to(cuda)).sum().backward()
+    g = d_p.grad.cpu().numpy().astype(np.float64)
+    g64 = O.image_grad(raw, p.astype(np.float64), window, O.LANCZOS, G.astype(np.float64), db=db)
+    scale = np.abs(g64).max()
+    assert np.all(np.abs(g - g64) <= 2e-2 * scale + 2e-2 * np.abs(g64)), (g, g64)
+
+
+@pytest.mark.gpu
+def test_entropy_gradient_matches_gpu_finite_differences(cuda):
+    raw_t, raw, window, ctrue = make_case(m=256, seed=11)
+    p = params_of(8.0, -6.0, np.asarray(ctrue) + np.array([0.0, 0.0, 2.0, -2.0]))
+    af = _af(cuda, O.LANCZOS, window)
+    d_raw = raw_t.to(cuda)
+    hs = torch.empty(2, dtype=torch.float64, device=cuda)
+    grad = torch.empty(8, dtype=torch.float32, device=cuda)
+    d_p = torch.from_numpy(p).to(cuda)
+    af.forward(d_raw, d_p, hs=hs)
+    af.backward(d_raw, d_p, grad, hs=hs)
+    g = grad.cpu().numpy().astype(np.float64)
+    h = 1e-3
+    fd = np.zeros(8)
+    for k in range(8):
+        for sgn in (1, -1):
+            q = p.astype(np.float64).copy()
+            q[k] += sgn * h
+            af.forward(d_raw, torch.from_numpy(q.astype(np.float32)).to(cuda), hs=hs)
+            fd[k] += sgn * hs[0].item() / (2 * h)
+    # the float32 parameter vector rounds p +- h; use the steps actually taken
+    steps = np.array([(np.float32(v + h) - np.float32(v - h)) for v in p.astype(np.float64)], np.float64)
+    fd = fd * (2 * h) / steps
+    # c0 and c1 shift and stretch the k axis, to which the image entropy is
+    # nearly invariant: their gradients are small residuals of large per-sample
+    # terms, while the float32 resampling positions (ulp 1.2e-4 near r = 2000,
+    # as the reference evaluates them) turn a 1e-3 step into a jittered one.
+    # Their adjoint is checked against the float64 gradient instead.
+    checked = np.array([1, 1, 1, 1, 0, 0, 1, 1], bool)
+    big = checked & (np.abs(g) > 0.05 * np.abs(g).max())
+    assert big.sum() >= 4
+    assert np.all(np.abs(fd[big] - g[big]) <= 0.05 * np.abs(g[big])), (fd, g)
+
+
+@pytest.mark.gpu
+def test_fit_recovers_hidden_dispersion(cuda):
+    from octproengine_b200.autofocus import fit_dispersion
+    rng = np.random.default_rng(2024)
+    d2, d3 = rng.uniform(-40, 40), rng.uniform(-20, 20)
+    raw_t, raw, window, ctrue = make_case(m=256, seed=13, d2=d2, d3=d3)
+    af = _af(cuda, O.LANCZOS, window)
+    res = fit_dispersion(af, raw_t.to(cuda), ctrue)
+    err = max(abs(res.d2 - d2) / max(abs(d2), 1.0), abs(res.d3 - d3) / max(abs(d3), 1.0))
+    assert err < 0.01, (res, d2, d3)
+
+
+@pytest.mark.gpu
+def test_grid_sweep_finds_the_nearest_grid_point(cuda):
+    from octproengine_b200.autofocus import grid_sweep
+    d2, d3 = 13.0, -6.5
+    raw_t, raw, window, ctrue = make_case(m=64, seed=17, d2=d2, d3=d3)
+    af = _af(cuda, O.LANCZOS, window)
+    res = grid_sweep(af, raw_t.to(cuda), ctrue, n2=17, n3=17)
+    assert abs(res.d2 - d2) <= 80.0 / 16 and abs(res.d3 - d3) <= 40.0 / 16, res
+
+
+@pytest.mark.gpu
+def test_rejects_bad_arguments(cuda):
+    from octproengine_b200 import capi
+    from octproengine_b200.autofocus import Autofocus
+    with pytest.raises(capi.B200Error):
+        Autofocus(3000, "uint16", O.LANCZOS)
+    af = Autofocus(N, "uint16", O.LANCZOS)
+    d_p = torch.zeros(8, dtype=torch.float32, device=cuda)
+    raw = torch.zeros((4, N), dtype=torch.int16, device=cuda)
+    with pytest.raises(capi.B200Error):
+        af.forward(raw, d_p)  # neither an image nor (H, S) requested
+    with pytest.raises(TypeError):
+        af.forward(raw.float(), d_p, hs=torch.empty(2, dtype=torch.float64, device=cuda))
