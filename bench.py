@@ -259,6 +259,93 @@ def autofocus_bench(dev, seeds=range(8), ascans=1024):
     }
 
 
+def batch_bench(dev, seed=3, count=32, steps=20):
+    """32 uneven buffers in one persistent launch replayed from a CUDA graph.
+
+    Buffers drawn from `seed`: N in {1024, 2048, 4096}, A-scan counts uniform
+    in [256, 2048], input uint8 / uint16 / float32, resampling linear / cubic /
+    Lanczos-8 and window Hann / Gauss / sine / flat-top per buffer, dispersion
+    on, log output. The autotuner picks pairs-per-team and the radix schedule
+    per length first. Reported: total A-scans/s of the one-launch batch, the
+    same buffers as sequential single-buffer launches, and per length the HBM
+    fraction of that length's buffers launched alone.
+    """
+    import torch
+    from octproengine_b200 import synth
+    from octproengine_b200.batch import Batch
+    from octproengine_b200.chain import ChainSpec, open_context, UINT8, UINT16, FLOAT32, LINEAR, CUBIC, \
+        LANCZOS, HANN, GAUSS, SINE, FLAT_TOP
+    rng = np.random.default_rng(seed)
+    names = {UINT8: "uint8", UINT16: "uint16", FLOAT32: "float32"}
+    bytes_in = {UINT8: 1, UINT16: 2, FLOAT32: 4}
+    bufs = []
+    for k in range(count):
+        n = int(rng.choice([1024, 2048, 4096]))
+        m = int(rng.integers(256, 2049))
+        dt = int(rng.choice([UINT8, UINT16, FLOAT32]))
+        interp = int(rng.choice([LINEAR, CUBIC, LANCZOS]))
+        win = int(rng.choice([HANN, GAUSS, SINE, FLAT_TOP]))
+        spec = ChainSpec(signal_length=n, ascans_per_bscan=m, input_dtype=dt, resampling=True, interpolation=interp,
+                         resampling_coeffs=synth.linearising_coeffs(n), windowing=True, window_type=win,
+                         window_center=0.5, window_fill=0.9, dispersion=True,
+                         dispersion_coeffs=synth.compensating_coeffs(12.0, -6.0), grayscale_min=0.0,
+                         grayscale_max=100.0, device=dev.index or 0)
+        x = synth.generate(synth.SynthParams(n=n, ascans=m, seed=1000 + k, dtype=names[dt]), device=dev)
+        o = torch.empty((m, n // 2), dtype=torch.float32, device=dev)
+        bufs.append((spec, open_context(spec), x, o))
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def items(sel):
+        return [(c, x.data_ptr(), o.data_ptr(), s.num_ascans) for s, c, x, o in sel]
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    batch = Batch(items(bufs))
+    batch.autotune(3)
+    tuning = {n: batch.tuning(n) for n in (1024, 2048, 4096)}
+    ms_graph = timed(lambda: batch.run_graph(sp), steps)
+    ms_seq = timed(lambda: [c.process_device(x.data_ptr(), o.data_ptr(), sp, num_ascans=s.num_ascans)
+                            for s, c, x, o in bufs], steps)
+    total = sum(s.num_ascans for s, _, _, _ in bufs)
+    peak = measured_peak()[0]
+    per_len = {}
+    for n in (1024, 2048, 4096):
+        sel = [b for b in bufs if b[0].signal_length == n]
+        if not sel:
+            continue
+        sub = Batch(items(sel))
+        sub.set_tuning(n, tuning[n][0], tuning[n][1])
+        ms = timed(lambda: sub.run_graph(sp), steps)
+        nbytes = sum(s.num_ascans * (n * bytes_in[s.input_dtype] + (n // 2) * 4) for s, _, _, _ in sel)
+        asc = sum(s.num_ascans for s, _, _, _ in sel)
+        per_len[str(n)] = {"buffers": len(sel), "ascans": asc, "ascans_per_s": asc / (ms / 1e3),
+                           "gbs": nbytes / (ms / 1e3) / 1e9, "hbm_frac": nbytes / (ms / 1e3) / 1e9 / peak,
+                           "pairs_per_team": tuning[n][0], "radix_schedule": tuning[n][1]}
+        sub.close()
+    batch.close()
+    for _, c, _, _ in bufs:
+        if c.synchronize() != 0:
+            raise RuntimeError("batched chain reported a device status")
+        c.close()
+    return {"workload": f"{count} buffers (seed {seed}): N in {{1024, 2048, 4096}}, A-scans U[256, 2048], "
+                        "uint8/uint16/float32, linear/cubic/Lanczos-8, Hann/Gauss/sine/flat-top, one persistent "
+                        "launch replayed from a CUDA graph",
+            "ascans": total, "value": total / (ms_graph / 1e3), "unit": "A-scans/s", "ms_per_batch": ms_graph,
+            "sequential_single_launches": {"value": total / (ms_seq / 1e3), "ms_per_batch": ms_seq},
+            "per_length": per_len, "gpu_launches_per_batch": 1}
+
+
 def run_ours(args):
     import torch
     from octproengine_b200 import synth
@@ -395,6 +482,9 @@ def run_ours(args):
     autofocus = None
     if world == 1 and not args.no_autofocus:
         autofocus = autofocus_bench(dev)
+    batched = None
+    if world == 1 and not args.no_batch:
+        batched = batch_bench(dev)
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -427,6 +517,8 @@ def run_ours(args):
     }
     if autofocus:
         line["autofocus"] = autofocus
+    if batched:
+        line["batched"] = batched
     if cpu_base:
         line["cpu_baseline"] = cpu_base
     print(json.dumps(line), flush=True)
@@ -442,6 +534,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autofocus", action="store_true", help="skip the autofocus fit-versus-sweep line")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-buffer line")
     ap.add_argument("--bscans", type=int, default=BSCANS, help="B-scans per buffer (profiling uses fewer)")
     ap.add_argument("--interp", default="cubic", choices=["linear", "cubic", "lanczos"])
     ap.add_argument("--kernel-only", action="store_true",

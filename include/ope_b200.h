@@ -239,6 +239,49 @@ OPE_B200_API int ope_b200_af_backward(ope_b200_af* af, const void* d_in, int64_t
                                       int32_t output_mode, const float* d_grad_out, const double* d_hs,
                                       float* d_grad_params, void* stream);
 
+/* ---- batched chain: many buffers of uneven geometry in ONE persistent launch.
+ *      No counterpart in the reference, whose backends process one IOBuffer of
+ *      one geometry per ProcessingBackend::process call (backend_interface.h:24).
+ *      Each buffer is described by a configured context (its
+ *      ProcessorConfiguration and curves, ope_b200_create + curve setters) and
+ *      gets exactly the chain ope_b200_process_device_n runs for it. ----
+ *
+ * Limits: N in {1024, 2048, 4096}; input UINT8, UINT16 or FLOAT32 (as float);
+ * FPN subtraction with a set or determined profile, but no FPN determination
+ * (no pending request, no continuous mode). A batch snapshots its contexts'
+ * tables at creation: re-create it after changing a context's curves or
+ * configuration. One launch of a batch at a time (launches are stream-ordered
+ * by the caller; plain launches also wait for the previous one). */
+typedef struct ope_b200_batch ope_b200_batch;
+typedef struct ope_b200_batch_item {
+    ope_b200_ctx* ctx;  /* the buffer's chain configuration               */
+    const void* d_in;   /* num_ascans x N raw samples, 16-byte aligned      */
+    float* d_out;       /* num_ascans x N/2 floats                          */
+    int64_t num_ascans; /* >= 1                                             */
+} ope_b200_batch_item;
+OPE_B200_API int ope_b200_batch_create(const ope_b200_batch_item* items, int32_t count, ope_b200_batch** out);
+OPE_B200_API void ope_b200_batch_destroy(ope_b200_batch* batch);
+OPE_B200_API const char* ope_b200_batch_last_error(const ope_b200_batch* batch);
+/* One persistent launch over every buffer of the batch, on `stream`. */
+OPE_B200_API int ope_b200_batch_run(ope_b200_batch* batch, void* stream);
+/* Same launch from a CUDA graph: the first call (and the first after a tuning
+ * change) captures it, later calls replay it. The graph keeps the buffer
+ * pointers of the batch. */
+OPE_B200_API int ope_b200_batch_run_graph(ope_b200_batch* batch, void* stream);
+/* Tuning per signal length n: pairs_per_team (pairs of A-scans each team of
+ * N/16 threads takes per grab; a CTA takes 2 x pairs_per_team x 4096/N A-scans)
+ * and radix_schedule (0: radix-16 passes then the short one, 1: short first;
+ * n = 4096 has only 0). Defaults: 4 and 0. */
+OPE_B200_API int ope_b200_batch_set_tuning(ope_b200_batch* batch, int32_t n, int32_t pairs_per_team,
+                                           int32_t radix_schedule);
+OPE_B200_API int ope_b200_batch_get_tuning(ope_b200_batch* batch, int32_t n, int32_t* pairs_per_team,
+                                           int32_t* radix_schedule, float* best_us);
+/* Autotuner: for every length in the batch, times each candidate
+ * (pairs_per_team in {1, 2, 4, 8, 16, 32} x the radix schedules) on the
+ * batch's own buffers of that length (`reps` timed launches each, CUDA
+ * events, best kept) and keeps the fastest. Overwrites the outputs. */
+OPE_B200_API int ope_b200_batch_autotune(ope_b200_batch* batch, int32_t reps);
+
 /* Test hook, no reference counterpart: the next launch of this context skips
  * its first input copy, so its bounded wait runs out after `timeout_us`; the
  * kernel then records a status that ope_b200_synchronize / process_host

@@ -121,6 +121,15 @@ SIGNATURES = {
     "ope_b200_af_last_error": (ctypes.c_char_p, [_P]),
     "ope_b200_af_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P]),
     "ope_b200_af_backward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P, _P]),
+    "ope_b200_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "ope_b200_batch_destroy": (None, [_P]),
+    "ope_b200_batch_last_error": (ctypes.c_char_p, [_P]),
+    "ope_b200_batch_run": (ctypes.c_int, [_P, _P]),
+    "ope_b200_batch_run_graph": (ctypes.c_int, [_P, _P]),
+    "ope_b200_batch_set_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "ope_b200_batch_get_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                                 ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]),
+    "ope_b200_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32]),
     "ope_b200_abi_version": (ctypes.c_int, []),
     "ope_b200_device_supported": (ctypes.c_int, [ctypes.c_int32]),
 }

@@ -121,9 +121,10 @@ __global__ void __launch_bounds__(N / 16, 3) af_forward_kernel(const AfArgs a) {
     AfForwardSink<N> sink;
     sink.args = &a;
     const long long npairs = (a.c.m + 1) / 2;
-    run_pairs<N, DT, INTERP>(a.c, 0, a.c.m, blockIdx.x, npairs, gridDim.x, smem, sink);
+    const CtaTeam tm;
+    run_pairs<N, DT, INTERP, 0>(tm, a.c, 0, a.c.m, blockIdx.x, npairs, gridDim.x, smem, sink);
     double s = sink.s, e = sink.e;
-    team_sum2<N / 16, double>(s, e, reinterpret_cast<double*>(smem + LY::OFF_SCAN));
+    team_sum2<N / 16, double>(tm, s, e, reinterpret_cast<double*>(smem + LY::OFF_SCAN));
     if (threadIdx.x == 0) {
         a.partial[2 * blockIdx.x] = s;
         a.partial[2 * blockIdx.x + 1] = e;
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
             float2 vals[16];
             SS sa, sb;
             phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
-            team_sum2<T, SS>(sa, sb, reinterpret_cast<SS*>(scan));
+            team_sum2<T, SS>(CtaTeam{}, sa, sb, reinterpret_cast<SS*>(scan));
             const float2 lvl = make_float2(split_level((double)sa, N, DT != IN_F32),
                                            split_level((double)sb, N, DT != IN_F32));
             phase_split_store<N>(t, vals, lvl, spec);

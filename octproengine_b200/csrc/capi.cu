@@ -281,6 +281,36 @@ static ChainArgs make_args(ope_b200_ctx* c, const void* d_in, float* d_out, long
     return a;
 }
 
+namespace ope_b200 {
+
+// Chain arguments of the context's current configuration for the batched
+// launcher (batch.cu): tables rebuilt if a curve changed, the fixed-pattern
+// profile if subtraction is on. Input, output and A-scan count are left for
+// the caller. FPN determination needs the per-buffer state machine of
+// process_locked and is not available to batches.
+int ctx_batch_args(ope_b200_ctx* c, ChainArgs* a, int* n, int* in_kind, int* interp, int* device) {
+    if (!c || !a) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    OPE_CU(c, cudaSetDevice(c->device));
+    if (c->tables_dirty) {
+        int rc = rebuild_tables(c);
+        if (rc != OPE_B200_OK) return rc;
+    }
+    if (c->fpn.requested || c->cfg.fpn_continuous)
+        return fail(c, OPE_B200_E_UNSUPPORTED, "FPN determination is not available in a batch");
+    const float2* fpn = (c->cfg.fpn_removal && c->fpn.valid) ? c->fpn.d_profile : nullptr;
+    *a = make_args(c, nullptr, nullptr, 0, fpn);
+    *n = c->n;
+    *in_kind = c->in_kind;
+    *interp = c->interp;
+    *device = c->device;
+    return OPE_B200_OK;
+}
+
+const char* ctx_error(const ope_b200_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+}  // namespace ope_b200
+
 extern "C" {
 
 int ope_b200_abi_version(void) { return OPE_B200_ABI_VERSION; }

@@ -66,10 +66,31 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
+// A team is the group of threads that processes one pair of A-scans.
+// CtaTeam: the whole CTA (barrier 0). SubTeam: `count` threads starting at
+// thread `base` (both multiples of 32), synchronised by named barrier `id`
+// (1..15), so several teams can share one CTA.
+struct CtaTeam {
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+struct SubTeam {
+    int base, id, count;
+    __device__ __forceinline__ int tid() const { return (int)threadIdx.x - base; }
+    __device__ __forceinline__ void sync() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+    }
+};
+
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Exclusive team scan of two values per thread (T threads, T % 32 == 0).
-template <int T, typename S>
-__device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+template <int T, typename S, class Team>
+__device__ __forceinline__ void team_exclusive_scan2(const Team& tm, S& a, S& b, S* scratch) {
+    const int lane = tm.tid() & 31, warp = tm.tid() >> 5;
     S ia = a, ib = b;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -84,7 +105,7 @@ __device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
         scratch[2 * warp] = ia;
         scratch[2 * warp + 1] = ib;
     }
-    __syncthreads();
+    tm.sync();
     S pa = 0, pb = 0;
     for (int w = 0; w < warp; ++w) {
         pa += scratch[2 * w];
@@ -96,9 +117,9 @@ __device__ __forceinline__ void team_exclusive_scan2(S& a, S& b, S* scratch) {
 
 // Team sum of two doubles, in a fixed order (xor butterfly inside each warp,
 // then warp totals in warp order) that the CPU emulation reproduces.
-template <int T, typename S>
-__device__ __forceinline__ void team_sum2(S& a, S& b, S* scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+template <int T, typename S, class Team>
+__device__ __forceinline__ void team_sum2(const Team& tm, S& a, S& b, S* scratch) {
+    const int lane = tm.tid() & 31, warp = tm.tid() >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -108,7 +129,7 @@ __device__ __forceinline__ void team_sum2(S& a, S& b, S* scratch) {
         scratch[2 * warp] = a;
         scratch[2 * warp + 1] = b;
     }
-    __syncthreads();
+    tm.sync();
     S ta = 0, tb = 0;
     for (int w = 0; w < T / 32; ++w) {
         ta += scratch[2 * w];
@@ -118,9 +139,9 @@ __device__ __forceinline__ void team_sum2(S& a, S& b, S* scratch) {
     b = tb;
 }
 
-template <int T>
-__device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+template <int T, class Team>
+__device__ __forceinline__ void team_minmax2(const Team& tm, float2& mn, float2& mx, float* scratch) {
+    const int lane = tm.tid() & 31, warp = tm.tid() >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mn.x = fminf(mn.x, __shfl_xor_sync(0xffffffffu, mn.x, o));
@@ -134,7 +155,7 @@ __device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scra
         scratch[4 * warp + 2] = mx.x;
         scratch[4 * warp + 3] = mx.y;
     }
-    __syncthreads();
+    tm.sync();
     mn = make_float2(scratch[0], scratch[1]);
     mx = make_float2(scratch[2], scratch[3]);
     for (int w = 1; w < T / 32; ++w) {
@@ -146,13 +167,13 @@ __device__ __forceinline__ void team_minmax2(float2& mn, float2& mx, float* scra
 }
 
 // Output stage for one pair: scaling, affine map, streaming stores.
-template <int N>
-__device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a, long long row_a, float2 dc,
-                                         float* scratch) {
-    using L = LastInfo<N>;
+template <int N, int S, class Team>
+__device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, const ChainArgs& a, long long row_a,
+                                         float2 dc, float* scratch) {
+    using L = LastInfo<N, S>;
     constexpr int NB = L::NB;
     float2 mag2[NB];
-    epi_mag2<N>(t, v, a, dc, mag2);
+    epi_mag2<N, S>(t, v, a, dc, mag2);
     float2 res[NB];
     if (a.log_mode) {
 #pragma unroll
@@ -169,7 +190,7 @@ __device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a,
                 mn = make_float2(fminf(mn.x, res[k].x), fminf(mn.y, res[k].y));
                 mx = make_float2(fmaxf(mx.x, res[k].x), fmaxf(mx.y, res[k].y));
             }
-            team_minmax2<Plan<N>::T>(mn, mx, scratch);
+            team_minmax2<Plan<N>::T>(tm, mn, mx, scratch);
             float ra = mx.x - mn.x, rb = mx.y - mn.y;
             if (!(ra >= 1e-6f)) ra = 1.0f;
             if (!(rb >= 1e-6f)) rb = 1.0f;
@@ -206,9 +227,12 @@ __device__ __forceinline__ void epilogue(int t, const cp* v, const ChainArgs& a,
 // < row_end), and hands each pair's bins to `sink(t, v, row_a, has_b)`.
 // Raw rows are staged by cp.async.bulk into a two-deep ring; every wait is
 // bounded (a.timeout_ns) and a timeout sets STATUS_MBAR_TIMEOUT and returns.
-template <int N, int DT, int INTERP, class Sink>
-__device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, long long row_end, long long p0,
-                                          long long p_end, long long step, unsigned char* smem, Sink& sink) {
+// `tm` is the team running the pairs (the CTA, or a named-barrier sub-team
+// whose shared-memory region starts at smem); S selects the radix schedule.
+template <int N, int DT, int INTERP, int S, class Team, class Sink>
+__device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, long long row0, long long row_end,
+                                          long long p0, long long p_end, long long step, unsigned char* smem,
+                                          Sink& sink) {
     using PL = Plan<N>;
     using LY = Layout<N, DT>;
     using sum_t = typename InTraits<DT>::sum_t;
@@ -224,7 +248,7 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + LY::OFF_MBAR);
     int* abort_flag = reinterpret_cast<int*>(smem + LY::OFF_MBAR + 16);
 
-    const int t = threadIdx.x;
+    const int t = tm.tid();
     constexpr uint32_t ROW_BYTES = N * sizeof(raw_t);
     const unsigned char* in = static_cast<const unsigned char*>(a.in);
 
@@ -234,7 +258,7 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
         fence_mbar_init();
         *abort_flag = 0;
     }
-    __syncthreads();
+    tm.sync();
 
     auto issue = [&](long long pair, int st) {
         const long long r = row0 + 2 * pair;
@@ -253,7 +277,7 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
         const long long nxt = item + step;
         if (t == 0 && nxt < p_end) issue(nxt, st ^ 1);
         if (!mbar_wait_bounded(&mbar[st], (it >> 1) & 1, a.timeout_ns)) *abort_flag = 1;
-        __syncthreads();
+        tm.sync();
         if (*abort_flag) {
             if (t == 0) {
                 if (a.status) atomicOr(a.status, STATUS_MBAR_TIMEOUT);
@@ -268,60 +292,61 @@ __device__ __forceinline__ void run_pairs(const ChainArgs& a, long long row0, lo
         if (a.dc_window > 0) {
             sum_t ta, tb;
             phase_dc_local<N, DT>(t, stage, &ta, &tb);
-            team_exclusive_scan2<T, sum_t>(ta, tb, scan);
+            team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan);
             phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
-            __syncthreads();
+            tm.sync();
             phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
         } else if (a.dc_resp) {
             using SS = typename SplitSum<DT>::type;
             float2 vals[16];
             SS sa, sb;
             phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
-            team_sum2<T, SS>(sa, sb, reinterpret_cast<SS*>(scan));
+            team_sum2<T, SS>(tm, sa, sb, reinterpret_cast<SS*>(scan));
             dc = make_float2(split_level((double)sa, N, DT != IN_F32), split_level((double)sb, N, DT != IN_F32));
             phase_split_store<N>(t, vals, dc, spec);
         } else {
             phase_unpack<N, DT>(t, stage, spec);
         }
-        __syncthreads();
+        tm.sync();
 
         // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];
         phase_prestage<N, INTERP>(t, spec, a, v);
-        fft_twiddle_dft<N, 0>(t, v, a.tw);
-        __syncthreads();  // spec aliases the exchange buffer
-        fft_store<N, 0>(t, v, exch);
-        __syncthreads();
+        fft_twiddle_dft<N, 0, false, S>(t, v, a.tw);
+        tm.sync();  // spec aliases the exchange buffer
+        fft_store<N, 0, S>(t, v, exch);
+        tm.sync();
         if constexpr (NPASS > 2) {
             fft_load<N>(t, exch, v);
-            fft_twiddle_dft<N, 1>(t, v, a.tw);
-            __syncthreads();
-            fft_store<N, 1>(t, v, exch);
-            __syncthreads();
+            fft_twiddle_dft<N, 1, false, S>(t, v, a.tw);
+            tm.sync();
+            fft_store<N, 1, S>(t, v, exch);
+            tm.sync();
         }
         if constexpr (NPASS > 3) {
             fft_load<N>(t, exch, v);
-            fft_twiddle_dft<N, 2>(t, v, a.tw);
-            __syncthreads();
-            fft_store<N, 2>(t, v, exch);
-            __syncthreads();
+            fft_twiddle_dft<N, 2, false, S>(t, v, a.tw);
+            tm.sync();
+            fft_store<N, 2, S>(t, v, exch);
+            tm.sync();
         }
         fft_load<N>(t, exch, v);
-        fft_twiddle_dft<N, NPASS - 1>(t, v, a.tw);
+        fft_twiddle_dft<N, NPASS - 1, false, S>(t, v, a.tw);
         const long long ra = row0 + 2 * item;
         sink(t, v, ra, ra + 1 < row_end, dc);
-        __syncthreads();  // next item overwrites spec/exch
+        tm.sync();  // next item overwrites spec/exch
     }
 }
 
-template <int N>
+template <int N, int S, class Team>
 struct ImageSink {
+    const Team& tm;
     const ChainArgs& a;
     float* scratch;
     __device__ __forceinline__ void operator()(int t, const cp* v, long long row_a, bool has_b, float2 dc) {
         if (a.bins_out) {
             // complex bins after the (optional) FPN subtraction, before magnitude
-            using L = LastInfo<N>;
+            using L = LastInfo<N, S>;
 #pragma unroll
             for (int i = 0; i < L::D; ++i)
 #pragma unroll
@@ -338,7 +363,7 @@ struct ImageSink {
                 }
             return;
         }
-        epilogue<N>(t, v, a, row_a, dc, scratch);
+        epilogue<N, S>(tm, t, v, a, row_a, dc, scratch);
     }
 };
 
@@ -346,9 +371,10 @@ template <int N, int DT, int INTERP>
 __global__ void __launch_bounds__(N / 16, 3) chain_kernel(const ChainArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     using LY = Layout<N, DT>;
-    ImageSink<N> sink{a, reinterpret_cast<float*>(smem + LY::OFF_SCAN)};
+    const CtaTeam tm;
+    ImageSink<N, 0, CtaTeam> sink{tm, a, reinterpret_cast<float*>(smem + LY::OFF_SCAN)};
     const long long npairs = (a.m + 1) / 2;
-    run_pairs<N, DT, INTERP>(a, 0, a.m, blockIdx.x, npairs, gridDim.x, smem, sink);
+    run_pairs<N, DT, INTERP, 0>(tm, a, 0, a.m, blockIdx.x, npairs, gridDim.x, smem, sink);
 }
 
 }  // namespace ope_b200
@@ -406,7 +432,7 @@ __global__ void __launch_bounds__(N / 16) fpn_stats_kernel(const ChainArgs a, lo
     sink.reset();
     if (hi > lo) {
         const long long npairs = (hi - lo + 1) / 2;
-        run_pairs<N, DT, INTERP>(a, lo, hi, blockIdx.x, npairs, gridDim.x, smem, sink);
+        run_pairs<N, DT, INTERP, 0>(CtaTeam{}, a, lo, hi, blockIdx.x, npairs, gridDim.x, smem, sink);
     }
     const int t = threadIdx.x;
     double* dst = partial + ((long long)s * gridDim.x + blockIdx.x) * (N / 2) * 3;

@@ -487,23 +487,45 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
 }
 
 // ------------------------------------------------------------- FFT passes --
-// Stockham pass p with radix R = 16 (or LASTR for the last pass), Ns = 16^p:
-// DFT d = t + i*T (i < D = 16/R) reads x[d + r*N/R] = slot s = i + r*D,
-// multiplies by W_{Ns R}^{r k} (k = d mod Ns), and writes output q to
-// (d - k)*R + k + q*Ns.
+// Stockham pass p with radix R and span NS (the product of the earlier
+// radices): DFT d = t + i*T (i < D = 16/R) reads x[d + r*N/R] = slot
+// s = i + r*D, multiplies by W_{NS R}^{r k} (k = d mod NS), and writes output
+// q to (d - k)*R + k + q*NS.
+//
+// Radix schedule S: every pass has radix 16 except one of radix LASTR
+// (N = 16^(NPASS-1) * LASTR); S = 0 runs that pass last, S = 1 first.
 
-template <int N, int P>
+template <int N, int S>
+struct Sched {
+    static_assert(S == 0 || S == 1, "radix schedule 0 (small radix last) or 1 (small radix first)");
+    static constexpr int NPASS = Plan<N>::NPASS;
+    static constexpr int radix(int p) {
+        return (S == 0) ? ((p == NPASS - 1) ? Plan<N>::LASTR : 16) : ((p == 0) ? Plan<N>::LASTR : 16);
+    }
+    static constexpr int span(int p) {
+        int v = 1;
+        for (int q = 0; q < p; ++q) v *= radix(q);
+        return v;
+    }
+    // Twiddles of pass p >= 1 live in one block of (R-1) x NS entries,
+    // entry (r-1)*NS + k = W_{NS*R}^{r*k}: threads with consecutive k read
+    // consecutive entries. Blocks of successive passes follow each other.
+    static constexpr int tw_off(int p) {
+        int o = 0;
+        for (int q = 1; q < p; ++q) o += (radix(q) - 1) * span(q);
+        return o;
+    }
+};
+
+template <int N, int P, int S = 0>
 struct PassInfo {
     static constexpr int NPASS = Plan<N>::NPASS;
     static constexpr bool LAST = (P == NPASS - 1);
-    static constexpr int R = LAST ? Plan<N>::LASTR : 16;
+    static constexpr int R = Sched<N, S>::radix(P);
     static constexpr int D = 16 / R;
-    static constexpr int NS = (P == 0) ? 1 : (P == 1) ? 16 : (P == 2) ? 256 : 4096;
-    // Twiddles of pass P >= 1 live in one block of (R-1) x NS entries,
-    // entry (r-1)*NS + k = W_{NS*R}^{r*k}: threads with consecutive k read
-    // consecutive entries. Blocks of successive passes follow each other.
+    static constexpr int NS = Sched<N, S>::span(P);
     static constexpr int TW_SIZE = (P == 0) ? 0 : (R - 1) * NS;
-    static constexpr int TW_OFF = (P <= 1) ? 0 : PassInfo<N, (P > 1 ? P - 1 : 0)>::TW_OFF + PassInfo<N, (P > 1 ? P - 1 : 0)>::TW_SIZE;
+    static constexpr int TW_OFF = Sched<N, S>::tw_off(P);
 };
 
 template <int N>
@@ -520,9 +542,9 @@ OPE_HD void fft_load(int t, const float4* exch, cp* v) {
 
 // FULL = true computes every output of the last pass (all N bins); by default
 // the last pass keeps only bins [0, N/2).
-template <int N, int P, bool FULL = false>
+template <int N, int P, bool FULL = false, int S = 0>
 OPE_HD void fft_twiddle_dft(int t, cp* v, const float2* tw) {
-    using PI = PassInfo<N, P>;
+    using PI = PassInfo<N, P, S>;
     constexpr int T = Plan<N>::T;
     constexpr int R = PI::R, D = PI::D, NS = PI::NS;
     constexpr int NOUT = (PI::LAST && !FULL) ? R / 2 : R;
@@ -555,9 +577,9 @@ OPE_HD void fft_twiddle_dft(int t, cp* v, const float2* tw) {
     }
 }
 
-template <int N, int P>
+template <int N, int P, int S = 0>
 OPE_HD void fft_store(int t, const cp* v, float4* exch) {
-    using PI = PassInfo<N, P>;
+    using PI = PassInfo<N, P, S>;
     constexpr int T = Plan<N>::T;
     constexpr int R = PI::R, D = PI::D, NS = PI::NS;
 #pragma unroll
@@ -592,9 +614,9 @@ OPE_HD float fsqrt(float x) {
 }
 
 // Bin b of the last pass lives in v[i + q*D] for b = (t + i*T) + q*N/R.
-template <int N>
+template <int N, int S = 0>
 struct LastInfo {
-    using PI = PassInfo<N, Plan<N>::NPASS - 1>;
+    using PI = PassInfo<N, Plan<N>::NPASS - 1, S>;
     static constexpr int R = PI::R, D = PI::D;
     static constexpr int NB = D * (R / 2);  // bins per thread
     OPE_HD static int bin(int t, int i, int q) { return t + i * Plan<N>::T + q * (N / R); }
@@ -612,9 +634,9 @@ OPE_HD cp add_dc(const ChainArgs& a, cp x, int bin, float2 c) {
 }
 
 // |X|^2 with the optional fixed-pattern subtraction (cpu_kernels.tpp:460-479).
-template <int N>
+template <int N, int S = 0>
 OPE_HD void epi_mag2(int t, const cp* v, const ChainArgs& a, float2 c, float2* mag2) {
-    using L = LastInfo<N>;
+    using L = LastInfo<N, S>;
 #pragma unroll
     for (int i = 0; i < L::D; ++i)
 #pragma unroll

@@ -13,9 +13,10 @@ namespace ope_b200 {
 // evaluated with the same float operations.
 float lanczos8(float x);
 
-// Twiddles of the Stockham passes, per pass a block of (R-1) x NS entries
-// W_N^(r k N/(NS R)) (see PassInfo::TW_OFF), evaluated in double and rounded once.
-std::vector<float2> build_twiddles(int n);
+// Twiddles of the Stockham passes of radix schedule `sched` (Sched<N, S>),
+// per pass a block of (R-1) x NS entries W_N^(r k N/(NS R)) (see
+// Sched::tw_off), evaluated in double and rounded once.
+std::vector<float2> build_twiddles(int n, int sched = 0);
 
 // kLinearizationLinear indices and fractions (cpu_kernels.tpp:95-110):
 // {n1 + SPEC_PAD, bits of float(nx - n1)}.
