@@ -10,6 +10,7 @@
 // cuda_backend.cu:784-828).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -99,6 +100,10 @@ struct ope_b200_ctx {
     // host-path buffers
     void* d_in = nullptr;
     float* d_out = nullptr;
+
+    // pipelined host path (ope_b200_process_host)
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    cudaEvent_t ev_pipe[16] = {};
 
     // test hook: next launch skips its first bulk copy and waits at most this long
     unsigned long long inject_stall_ns = 0;
@@ -400,6 +405,16 @@ void ope_b200_destroy(ope_b200_ctx* c) {
         if (r.stream) cudaStreamDestroy(r.stream);
     }
     if (c->ev_last_compute) cudaEventDestroy(c->ev_last_compute);
+    if (c->s_h2d) {
+        cudaStreamSynchronize(c->s_h2d);
+        cudaStreamDestroy(c->s_h2d);
+    }
+    if (c->s_d2h) {
+        cudaStreamSynchronize(c->s_d2h);
+        cudaStreamDestroy(c->s_d2h);
+    }
+    for (auto& e : c->ev_pipe)
+        if (e) cudaEventDestroy(e);
     for (auto& s : c->slot) free_slot(s);
     cudaFree(c->d_tw);
     cudaFree(c->d_status);
@@ -528,11 +543,51 @@ int ope_b200_process_host(ope_b200_ctx* c, const void* h_in, float* h_out) {
     OPE_CU(c, cudaSetDevice(c->device));
     if (!c->d_in) OPE_CU(c, cudaMalloc(&c->d_in, c->in_bytes));
     if (!c->d_out) OPE_CU(c, cudaMalloc(&c->d_out, c->out_bytes));
-    OPE_CU(c, cudaMemcpyAsync(c->d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, c->stream));
-    int rc = process_locked(c, c->d_in, c->d_out, c->m, c->stream);
-    if (rc != OPE_B200_OK) return rc;
-    OPE_CU(c, cudaMemcpyAsync(h_out, c->d_out, c->out_bytes, cudaMemcpyDeviceToHost, c->stream));
-    OPE_CU(c, cudaStreamSynchronize(c->stream));
+    // Pipelined in chunks of whole B-scan pairs: the copy in of chunk k+1 and
+    // the copy out of chunk k-1 (two copy engines) overlap the chain on chunk
+    // k. Chunks start at even B-scans so the B-scan flip sees the same
+    // parities; FPN determination needs the whole buffer and runs unchunked.
+    const long long A = c->cfg.ascans_per_bscan;
+    const long long B = c->cfg.bscans_per_buffer;
+    const long long kChunks = 8;
+    const long long bs_per_chunk = 2 * ((B + 2 * kChunks - 1) / (2 * kChunks));
+    const bool chunked = !(c->fpn.requested || c->cfg.fpn_continuous) && B >= 4;
+    if (!chunked) {
+        OPE_CU(c, cudaMemcpyAsync(c->d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, c->stream));
+        int rc = process_locked(c, c->d_in, c->d_out, c->m, c->stream);
+        if (rc != OPE_B200_OK) return rc;
+        OPE_CU(c, cudaMemcpyAsync(h_out, c->d_out, c->out_bytes, cudaMemcpyDeviceToHost, c->stream));
+        OPE_CU(c, cudaStreamSynchronize(c->stream));
+    } else {
+        if (!c->s_h2d) OPE_CU(c, cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking));
+        if (!c->s_d2h) OPE_CU(c, cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking));
+        for (int k = 0; k < 2 * kChunks; ++k)
+            if (!c->ev_pipe[k]) OPE_CU(c, cudaEventCreateWithFlags(&c->ev_pipe[k], cudaEventDisableTiming));
+        const size_t in_row = c->in_bytes / static_cast<size_t>(c->m);
+        const size_t out_row = static_cast<size_t>(c->n / 2) * sizeof(float);
+        int k = 0;
+        for (long long b0 = 0; b0 < B; b0 += bs_per_chunk, ++k) {
+            const long long r0 = b0 * A;
+            const long long rows = std::min(bs_per_chunk, B - b0) * A;
+            const unsigned char* src = static_cast<const unsigned char*>(h_in) + r0 * in_row;
+            unsigned char* din = static_cast<unsigned char*>(c->d_in) + r0 * in_row;
+            float* dout = c->d_out + r0 * (c->n / 2);
+            OPE_CU(c, cudaMemcpyAsync(din, src, rows * in_row, cudaMemcpyHostToDevice, c->s_h2d));
+            OPE_CU(c, cudaEventRecord(c->ev_pipe[2 * k], c->s_h2d));
+            OPE_CU(c, cudaStreamWaitEvent(c->stream, c->ev_pipe[2 * k], 0));
+            int rc = process_locked(c, din, dout, rows, c->stream);
+            if (rc != OPE_B200_OK) {
+                cudaStreamSynchronize(c->s_h2d);
+                cudaStreamSynchronize(c->s_d2h);
+                return rc;
+            }
+            OPE_CU(c, cudaEventRecord(c->ev_pipe[2 * k + 1], c->stream));
+            OPE_CU(c, cudaStreamWaitEvent(c->s_d2h, c->ev_pipe[2 * k + 1], 0));
+            OPE_CU(c, cudaMemcpyAsync(h_out + r0 * (c->n / 2), dout, rows * out_row, cudaMemcpyDeviceToHost, c->s_d2h));
+        }
+        OPE_CU(c, cudaStreamSynchronize(c->s_d2h));
+        OPE_CU(c, cudaStreamSynchronize(c->stream));
+    }
     int st = 0;
     OPE_CU(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (st != 0) {

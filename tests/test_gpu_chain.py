@@ -212,3 +212,21 @@ def test_process_host_roundtrip(cuda):
         ctx.close()
     b = H.gpu_run(spec, raw)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("bscans,flip", [(7, True), (20, False), (4, True)])
+def test_pipelined_process_host_matches_device_path(cuda, bscans, flip):
+    # process_host splits buffers of >= 4 B-scans into chunks of B-scan pairs
+    # whose copies overlap the chain; every output bit must match one launch
+    spec = spec_for(1024, LANCZOS, m=16).with_(bscans_per_buffer=bscans, bscan_flip=flip, fpn_removal=True)
+    raw = H.random_raw(spec, seed=bscans)
+    prof = np.random.default_rng(2).normal(0, 500, 1024).astype(np.float32)
+    ctx = open_context(spec)
+    try:
+        ctx.set_fpn_profile(prof)
+        a = ctx.process_host(raw)
+        assert ctx.synchronize() == 0
+    finally:
+        ctx.close()
+    b = H.gpu_run(spec, raw, fpn_profile=prof)
+    assert np.array_equal(a, b)
