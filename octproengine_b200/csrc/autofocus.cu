@@ -26,8 +26,8 @@ __device__ __forceinline__ int af_trunc(float v) {
 }
 
 __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ params,
-                                 const float* __restrict__ window, int2* lin, int4* cub, int* lzb, float* lzw,
-                                 float* lzdw, float* rmask, float4* wph) {
+                                 const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
+                                 float* lzdw, float* rmask, float2* wph) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     // resampling position (processorconfiguration.cpp:438-459)
@@ -50,9 +50,8 @@ __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ pa
         const int i1 = af_trunc(nx);
         const int n1r = cl(i1);
         const int q0 = cl(abs(i1 - 1)) + SPEC_PAD, q1 = n1r + SPEC_PAD;
-        const int q2 = cl(i1 + 1) + SPEC_PAD, q3 = cl(i1 + 2) + SPEC_PAD;
         const float pos = __fsub_rn(nx, (float)n1r);
-        cub[j] = make_int4(q0 | (q1 << 16), q2 | (q3 << 16), __float_as_int(pos), __float_as_int(__fmul_rn(pos, pos)));
+        cub[j] = make_int2(q0 | (q1 << 16), __float_as_int(pos));
     } else if (interp == INTERP_LANCZOS) {
         const int n0 = af_trunc(nx);
         int b = n0 < -9 ? -9 : (n0 > n + 7 ? n + 7 : n0);
@@ -69,7 +68,7 @@ __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ pa
     sincosf(ph, &sn, &cs);
     const double w = window ? (double)window[j] : 1.0;
     const float wc = (float)(w * (double)cs), ws = (float)(w * (double)sn);
-    wph[j] = make_float4(wc, wc, ws, ws);
+    wph[j] = make_float2(wc, ws);
 }
 
 // Lanczos-8 tap weights of every output sample, one thread per (tap, sample);
@@ -149,12 +148,12 @@ struct ope_b200_af {
     float2* tw = nullptr;
     float2* dc_zero = nullptr;
     int2* lin = nullptr;
-    int4* cub = nullptr;
+    int2* cub = nullptr;
     int* lzb = nullptr;
     float* lzw = nullptr;
     float* lzdw = nullptr;
     float* rmask = nullptr;
-    float4* wph = nullptr;
+    float2* wph = nullptr;
     double* partial = nullptr;
     int cap = 0;
     std::string err;
@@ -278,12 +277,12 @@ int ope_b200_af_create(int32_t n, int32_t input_dtype, int32_t interpolation, co
     if ((e = cudaMalloc(&o->tw, nn * 8)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->dc_zero, nn / 2 * 8)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->lin, nn * 8)) != cudaSuccess) return bail(e);
-    if ((e = cudaMalloc(&o->cub, nn * 16)) != cudaSuccess) return bail(e);
+    if ((e = cudaMalloc(&o->cub, nn * 8)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->lzb, nn * 4)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->lzw, nn * 16 * 4)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->lzdw, nn * 16 * 4)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->rmask, nn * 4)) != cudaSuccess) return bail(e);
-    if ((e = cudaMalloc(&o->wph, nn * 16)) != cudaSuccess) return bail(e);
+    if ((e = cudaMalloc(&o->wph, nn * 8)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&o->partial, static_cast<size_t>(o->cap) * AF_NPARAM * 8)) != cudaSuccess) return bail(e);
     std::vector<float> w(nn, 1.0f);
     if (window) w.assign(window, window + nn);

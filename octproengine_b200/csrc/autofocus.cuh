@@ -76,8 +76,8 @@ __device__ __forceinline__ float af_lanczos8_deriv(float xf) {
 // (processorconfiguration.cpp:438-482): float Horner in j with the
 // coefficients divided by (N-1)^m, every operation rounded separately.
 __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ params,
-                                 const float* __restrict__ window, int2* lin, int4* cub, int* lzb, float* lzw,
-                                 float* lzdw, float* rmask, float4* wph);
+                                 const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
+                                 float* lzdw, float* rmask, float2* wph);
 
 // ------------------------------------------------------------ forward ----
 
@@ -156,10 +156,10 @@ __device__ __forceinline__ void af_interp_deriv(const float2* spec, const AfArgs
         y = fma2(dy, dup2(fr), y1);
     } else if (INTERP == INTERP_CUBIC) {
         // y = y1 + pos/2 (cc + cb pos + ca pos^2); dy/dpos = cc/2 + cb pos + 3/2 ca pos^2
-        const int4 e = a.c.cub[j];
-        const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16, i2 = e.y & 0xFFFF, i3 = (unsigned)e.y >> 16;
-        const float pos = __int_as_float(e.z);
-        const float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i2], y3 = spec[i3];
+        const int2 e = a.c.cub[j];
+        const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
+        const float pos = __int_as_float(e.y);
+        const float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i1 + 1], y3 = spec[i1 + 2];
         const float2 ca = add2(sub2(mul2(dup2(3.0f), sub2(y1, y2)), y0), y3);
         const float2 cb = sub2(add2(sub2(mul2(dup2(2.0f), y0), mul2(dup2(5.0f), y1)), mul2(dup2(4.0f), y2)), y3);
         const float2 cc = sub2(y2, y0);
@@ -346,8 +346,8 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
             for (int q = 0; q < PI::R; ++q) {
                 const int j = t + i * T + q * (N / PI::R);
                 const cp A = v[i + q * PI::D];
-                const float4 w = __ldg(c.wph + j);
-                const float2 wc = make_float2(w.x, w.y), ws = make_float2(w.z, w.w);
+                const float2 w = __ldg(c.wph + j);
+                const float2 wc = dup2(w.x), ws = dup2(w.y);
                 const float2 hre = fma2(A.re, wc, neg2(mul2(A.im, ws)));
                 const float2 him = fma2(A.re, ws, mul2(A.im, wc));
                 float2 y, dy;

@@ -62,10 +62,10 @@ int input_kind(int dt, bool float_as_uint) {
 
 struct TableSlot {
     int2* lin = nullptr;
-    int4* cub = nullptr;
+    int2* cub = nullptr;
     int* lzb = nullptr;
     float* lzw = nullptr;
-    float4* wph = nullptr;
+    float2* wph = nullptr;
     float2* dcr = nullptr;  // DC response for the exact DC split (n/2)
     bool has_dcr = false;
     cudaEvent_t last_use = nullptr;
@@ -207,8 +207,8 @@ int rebuild_tables(ope_b200_ctx* c) {
             OPE_CU(c, cudaMemcpy(s.lin, tab.data(), n * sizeof(int2), cudaMemcpyHostToDevice));
             c->interp = INTERP_LINEAR;
         } else if (method == 1) {
-            std::vector<int4> tab = build_cubic_table(c->resample.data(), n);
-            OPE_CU(c, cudaMemcpy(s.cub, tab.data(), n * sizeof(int4), cudaMemcpyHostToDevice));
+            std::vector<int2> tab = build_cubic_table(c->resample.data(), n);
+            OPE_CU(c, cudaMemcpy(s.cub, tab.data(), n * sizeof(int2), cudaMemcpyHostToDevice));
             c->interp = INTERP_CUBIC;
         } else {
             std::vector<int> base;
@@ -226,8 +226,8 @@ int rebuild_tables(ope_b200_ctx* c) {
         return fail(c, OPE_B200_E_STATE, "windowing enabled but no window curve of length N was set");
     // dispersionCompensation skips when the phase length differs from N (cpu_kernels.tpp:205-208)
     const bool disp = cfg.dispersion_enabled && c->cos_sin.size() == 2 * static_cast<size_t>(n);
-    std::vector<float4> wph = build_window_phase(win ? c->window.data() : nullptr, disp ? c->cos_sin.data() : nullptr, n);
-    OPE_CU(c, cudaMemcpy(s.wph, wph.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    std::vector<float2> wph = build_window_phase(win ? c->window.data() : nullptr, disp ? c->cos_sin.data() : nullptr, n);
+    OPE_CU(c, cudaMemcpy(s.wph, wph.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
     // exact DC split: not needed when the rolling-average DC removal is on
     s.has_dcr = cfg.dc_split && !cfg.dc_removal_enabled;
     if (s.has_dcr) {
@@ -244,10 +244,10 @@ int rebuild_tables(ope_b200_ctx* c) {
 int alloc_slot(ope_b200_ctx* c, TableSlot& s) {
     const size_t n = static_cast<size_t>(c->n);
     OPE_CU(c, cudaMalloc(&s.lin, n * sizeof(int2)));
-    OPE_CU(c, cudaMalloc(&s.cub, n * sizeof(int4)));
+    OPE_CU(c, cudaMalloc(&s.cub, n * sizeof(int2)));
     OPE_CU(c, cudaMalloc(&s.lzb, n * sizeof(int)));
     OPE_CU(c, cudaMalloc(&s.lzw, 16 * n * sizeof(float)));
-    OPE_CU(c, cudaMalloc(&s.wph, n * sizeof(float4)));
+    OPE_CU(c, cudaMalloc(&s.wph, n * sizeof(float2)));
     OPE_CU(c, cudaMalloc(&s.dcr, (n / 2) * sizeof(float2)));
     OPE_CU(c, cudaEventCreateWithFlags(&s.last_use, cudaEventDisableTiming));
     return OPE_B200_OK;

@@ -367,8 +367,10 @@ struct ImageSink {
     }
 };
 
+// Register cap 128 per thread for every length (8192/N CTAs of N/16 threads
+// fill the register file): 16 warps per SM where shared memory allows.
 template <int N, int DT, int INTERP>
-__global__ void __launch_bounds__(N / 16, 3) chain_kernel(const ChainArgs a) {
+__global__ void __launch_bounds__(N / 16, 8192 / N) chain_kernel(const ChainArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     using LY = Layout<N, DT>;
     const CtaTeam tm;

@@ -54,10 +54,10 @@ struct ChainArgs {
     long long m;         // A-scans in this buffer
     const float2* tw;    // W_N^j = (cos, sin)(2 pi j / N), j < N
     const int2* lin;     // LINEAR: {n1 + PAD, float bits of (nx - n1)}
-    const int4* cub;     // CUBIC: {n0|n1<<16, n2|n3<<16 (all +PAD), pos bits, pos^2 bits}
+    const int2* cub;     // CUBIC: {n0 | n1<<16 (both +PAD), pos bits}; taps n2, n3 are n1+1, n1+2
     const int* lz_base;  // LANCZOS: first tap index + PAD
     const float* lz_w;   // LANCZOS: 16 x N tap weights, tap-major
-    const float4* wph;   // {w*cos, w*cos, w*sin, w*sin} (window folded into the phase)
+    const float2* wph;   // {w*cos, w*sin} (window folded into the phase)
     const float2* fpn;   // N/2 complex fixed-pattern profile, or nullptr
     int dc_window;       // rolling-average half window W; 0 = off
     int log_mode;        // 1: logarithmic, 0: linear
@@ -439,11 +439,15 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
             y = add2(y1, mul2x(sub2(y2, y1), dup2(fr), NZ));
         } else if (INTERP == INTERP_CUBIC) {
             // kLinearizationCubic + cubicHermiteInterpolation (cpu_kernels.tpp:124-145,486-502)
-            int4 e = a.cub[j];
-            int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16, i2 = e.y & 0xFFFF, i3 = (unsigned)e.y >> 16;
-            OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 < N + 2 * SPEC_PAD && i2 < N + 2 * SPEC_PAD && i3 < N + 2 * SPEC_PAD);
-            const float pos = bits_f(e.z), pos2 = bits_f(e.w);
-            float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i2], y3 = spec[i3];
+#if defined(__CUDA_ARCH__)
+            const int2 e = __ldg(a.cub + j);
+#else
+            const int2 e = a.cub[j];
+#endif
+            const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
+            OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 + 2 < N + 2 * SPEC_PAD);
+            const float pos = bits_f(e.y), pos2 = fmul_rn(pos, pos);
+            float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i1 + 1], y3 = spec[i1 + 2];
             float2 ca = add2(sub2(mul2x(dup2(3.0f), sub2(y1, y2), NZ), y0), y3);
             float2 cb = sub2(add2(sub2(mul2x(dup2(2.0f), y0, NZ), mul2x(dup2(5.0f), y1, NZ)),
                                   mul2x(dup2(4.0f), y2, NZ)),
@@ -475,14 +479,14 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
 #endif
         // applyWindow then dispersionCompensation (cpu_kernels.tpp:198-235):
         // re = y*w*cos, im = y*w*sin with the window folded into the phase
-        // factors (w*cos, w*sin), evaluated in double and rounded once; the
-        // table holds each factor twice, one per lane.
+        // factors (w*cos, w*sin), evaluated in double and rounded once and
+        // shared by both lanes.
 #if defined(__CUDA_ARCH__)
-        const float4 q = __ldg(a.wph + j);
+        const float2 q = __ldg(a.wph + j);
 #else
-        const float4 q = a.wph[j];
+        const float2 q = a.wph[j];
 #endif
-        v[s] = cpmake(mul2x(y, make_float2(q.x, q.y), NZ), mul2x(y, make_float2(q.z, q.w), NZ));
+        v[s] = cpmake(mul2x(y, dup2(q.x), NZ), mul2x(y, dup2(q.y), NZ));
     }
 }
 

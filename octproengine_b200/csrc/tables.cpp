@@ -79,8 +79,8 @@ std::vector<int2> build_linear_table(const float* curve, int n) {
     return tab;
 }
 
-std::vector<int4> build_cubic_table(const float* curve, int n) {
-    std::vector<int4> tab(n);
+std::vector<int2> build_cubic_table(const float* curve, int n) {
+    std::vector<int2> tab(n);
     auto cl = [n](int v) {
         if (v > n - 1) v = n - 1;
         if (v < -SPEC_PAD) v = -SPEC_PAD;
@@ -89,14 +89,14 @@ std::vector<int4> build_cubic_table(const float* curve, int n) {
     for (int j = 0; j < n; ++j) {
         const float nx = curve[j];
         const int i1 = trunc_index(nx);
+        // taps n2 = min(i1+1, n-1) and n3 = min(i1+2, n-1) are read as n1+1 and
+        // n1+2: past n-1 (or below 0) the replicated-edge padding holds the
+        // clamped sample, so only n0 = |i1-1| needs its own index
         const int n0 = cl(std::abs(i1 - 1)) + SPEC_PAD;
         const int n1r = cl(i1);
         const int n1 = n1r + SPEC_PAD;
-        const int n2 = cl(i1 + 1) + SPEC_PAD;
-        const int n3 = cl(i1 + 2) + SPEC_PAD;
         const float pos = nx - static_cast<float>(n1r);
-        const float pos2 = pos * pos;
-        tab[j] = make_int4(n0 | (n1 << 16), n2 | (n3 << 16), float_bits(pos), float_bits(pos2));
+        tab[j] = make_int2(n0 | (n1 << 16), float_bits(pos));
     }
     return tab;
 }
@@ -178,13 +178,13 @@ std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w,
     return d;
 }
 
-std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n) {
-    std::vector<float4> t(n);
+std::vector<float2> build_window_phase(const float* window, const float* cos_sin, int n) {
+    std::vector<float2> t(n);
     for (int j = 0; j < n; ++j) {
         const double w = window ? static_cast<double>(window[j]) : 1.0;
         const float wc = static_cast<float>(w * (cos_sin ? static_cast<double>(cos_sin[2 * j]) : 1.0));
         const float ws = static_cast<float>(w * (cos_sin ? static_cast<double>(cos_sin[2 * j + 1]) : 0.0));
-        t[j] = make_float4(wc, wc, ws, ws);
+        t[j] = make_float2(wc, ws);
     }
     return t;
 }

@@ -22,9 +22,10 @@ std::vector<float2> build_twiddles(int n, int sched = 0);
 // {n1 + SPEC_PAD, bits of float(nx - n1)}.
 std::vector<int2> build_linear_table(const float* curve, int n);
 
-// kLinearizationCubic indices (cpu_kernels.tpp:124-145), packed 16-bit and
-// offset by SPEC_PAD, plus pos and pos*pos as float bits.
-std::vector<int4> build_cubic_table(const float* curve, int n);
+// kLinearizationCubic indices (cpu_kernels.tpp:124-145): n0 and n1, packed
+// 16-bit and offset by SPEC_PAD, and pos as float bits (the kernel reads taps
+// n1+1, n1+2 and forms pos*pos).
+std::vector<int2> build_cubic_table(const float* curve, int n);
 
 // kLinearizationLanczos taps (cpu_kernels.tpp:176-195): per output index the
 // first gathered index (+ SPEC_PAD) and 16 weights (tap-major, 16 x n).
@@ -37,10 +38,9 @@ void build_lanczos_table(const float* curve, int n, std::vector<int>& base, std:
 std::vector<float2> build_dc_response(int n, int interp, const float* lanczos_w, const float* window,
                                       const float* cos_sin);
 
-// {w cos, w cos, w sin, w sin} per sample (each factor once per lane of a
-// pair), products in double rounded once; a missing window is 1, a missing
-// phase (cos 1, sin 0).
-std::vector<float4> build_window_phase(const float* window, const float* cos_sin, int n);
+// {w cos, w sin} per sample, products in double rounded once; a missing
+// window is 1, a missing phase (cos 1, sin 0).
+std::vector<float2> build_window_phase(const float* window, const float* cos_sin, int n);
 
 // Output affine constants of logScaleAndTruncate / linearScaleAndTruncate
 // (cpu_kernels.tpp:301-378) folded for the kernel epilogue.

@@ -50,13 +50,13 @@ int emu_run(const EmuArgs& e, int what, float* out) {
 
     std::vector<float2> tw = build_twiddles(N);
     std::vector<int2> lin;
-    std::vector<int4> cub;
+    std::vector<int2> cub;
     std::vector<int> lzb;
     std::vector<float> lzw;
     if (INTERP == INTERP_LINEAR) lin = build_linear_table(e.curve, N);
     if (INTERP == INTERP_CUBIC) cub = build_cubic_table(e.curve, N);
     if (INTERP == INTERP_LANCZOS) build_lanczos_table(e.curve, N, lzb, lzw);
-    std::vector<float4> wph = build_window_phase(e.window, e.cos_sin, N);
+    std::vector<float2> wph = build_window_phase(e.window, e.cos_sin, N);
     std::vector<float2> dcr;
     if (e.dc_split && e.dc_window == 0)
         dcr = build_dc_response(N, INTERP, lzw.empty() ? nullptr : lzw.data(), e.window, e.cos_sin);
