@@ -68,7 +68,6 @@ __device__ __noinline__ void batch_team_run(const BatchDesc& d, long long u, uns
     if (tm.tid() == 0) {  // the region may hold another layout in the next unit
         uint64_t* mbar = reinterpret_cast<uint64_t*>(my + Layout<N, DT>::OFF_MBAR);
         mbar_inval(&mbar[0]);
-        mbar_inval(&mbar[1]);
     }
 }
 
@@ -89,7 +88,7 @@ __device__ __forceinline__ void dispatch_dt_interp(const BatchDesc& d, long long
 #undef OPE_B200_BATCH_INTERP
 }
 
-__global__ void __launch_bounds__(BATCH_THREADS, 1)
+__global__ void __launch_bounds__(BATCH_THREADS, 2)
     batch_kernel(const BatchDesc* __restrict__ descs, int ndesc, long long total_units, unsigned long long* counter) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(16) BatchDesc sd;

@@ -225,8 +225,10 @@ __device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, con
 // Runs the chain up to the last FFT pass for the pairs p = p0, p0 + step, ...
 // (< p_end) whose rows are row0 + 2p and row0 + 2p + 1 (the second one only if
 // < row_end), and hands each pair's bins to `sink(t, v, row_a, has_b)`.
-// Raw rows are staged by cp.async.bulk into a two-deep ring; every wait is
-// bounded (a.timeout_ns) and a timeout sets STATUS_MBAR_TIMEOUT and returns.
+// Raw rows are staged by cp.async.bulk into one shared-memory stage: the copy
+// of the next pair is issued as soon as this pair's rows are unpacked, so it
+// overlaps the resampling, the DFT and the epilogue. Every wait is bounded
+// (a.timeout_ns) and a timeout sets STATUS_MBAR_TIMEOUT and returns.
 // `tm` is the team running the pairs (the CTA, or a named-barrier sub-team
 // whose shared-memory region starts at smem); S selects the radix schedule.
 template <int N, int DT, int INTERP, int S, class Team, class Sink>
@@ -254,38 +256,34 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
 
     if (t == 0) {
         mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
         fence_mbar_init();
         *abort_flag = 0;
     }
     tm.sync();
 
-    auto issue = [&](long long pair, int st) {
+    auto issue = [&](long long pair) {
         const long long r = row0 + 2 * pair;
         const uint32_t rows = (row_end - r) >= 2 ? 2u : 1u;
         const uint32_t bytes = rows * ROW_BYTES;
         fence_proxy_async_smem();
-        mbar_expect_tx(&mbar[st], bytes);
-        bulk_g2s(stages + st * LY::STAGE_BYTES, in + r * (long long)ROW_BYTES, bytes, &mbar[st]);
+        mbar_expect_tx(&mbar[0], bytes);
+        bulk_g2s(stages, in + r * (long long)ROW_BYTES, bytes, &mbar[0]);
     };
 
     long long item = p0;
-    if (t == 0 && item < p_end && !a.debug_skip_first_copy) issue(item, 0);
+    if (t == 0 && item < p_end && !a.debug_skip_first_copy) issue(item);
 
     for (int it = 0; item < p_end; item += step, ++it) {
-        const int st = it & 1;
         const long long nxt = item + step;
-        if (t == 0 && nxt < p_end) issue(nxt, st ^ 1);
-        if (!mbar_wait_bounded(&mbar[st], (it >> 1) & 1, a.timeout_ns)) *abort_flag = 1;
+        if (!mbar_wait_bounded(&mbar[0], it & 1, a.timeout_ns)) *abort_flag = 1;
         tm.sync();
         if (*abort_flag) {
-            if (t == 0) {
-                if (a.status) atomicOr(a.status, STATUS_MBAR_TIMEOUT);
-                if (nxt < p_end) (void)mbar_wait_bounded(&mbar[st ^ 1], ((it + 1) >> 1) & 1, a.timeout_ns);
-            }
+            // nothing else is in flight: the next copy is only issued after a
+            // successful wait
+            if (t == 0 && a.status) atomicOr(a.status, STATUS_MBAR_TIMEOUT);
             return;
         }
-        const unsigned char* stage = stages + st * LY::STAGE_BYTES;
+        const unsigned char* stage = stages;
 
         // ---- unpack (+ DC removal or exact DC split) ----
         float2 dc = make_float2(0.0f, 0.0f);
@@ -308,6 +306,7 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
             phase_unpack<N, DT>(t, stage, spec);
         }
         tm.sync();
+        if (t == 0 && nxt < p_end) issue(nxt);  // every thread is done with the stage
 
         // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];

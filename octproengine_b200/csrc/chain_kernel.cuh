@@ -134,7 +134,7 @@ struct Layout {
     static constexpr int OFF_SCAN = SPEC_BYTES + PFX_BYTES;  // 256 B of scan scratch
     static constexpr int OFF_EXCH = 0;
     static constexpr int OFF_STAGE = ((WORK_BYTES + 127) / 128) * 128;
-    static constexpr int OFF_MBAR = OFF_STAGE + 2 * STAGE_BYTES;
+    static constexpr int OFF_MBAR = OFF_STAGE + STAGE_BYTES;  // one stage: refilled once unpacked
     static constexpr int TOTAL = OFF_MBAR + 64;
 };
 
