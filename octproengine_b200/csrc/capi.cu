@@ -25,6 +25,7 @@
 #include "../../include/ope_b200.h"
 #include "chain_launch.h"
 #include "fpn.h"
+#include "postproc.h"
 #include "tables.h"
 
 using namespace ope_b200;
@@ -93,9 +94,13 @@ struct ope_b200_ctx {
     // fixed-pattern noise
     FpnState fpn;
 
-    // post-process background
+    // post-process background (profile on the device; the host copy is
+    // refreshed lazily after a recording)
     std::vector<float> bg_profile;
     bool bg_record_requested = false;
+    float* d_bg = nullptr;   // profile, n/2
+    float* d_bgv = nullptr;  // weight * profile + offset, n/2
+    bool bg_valid = false, bgv_dirty = true, bg_host_stale = false;
 
     // host-path buffers
     void* d_in = nullptr;
@@ -305,6 +310,18 @@ int ctx_batch_args(ope_b200_ctx* c, ChainArgs* a, int* n, int* in_kind, int* int
         return fail(c, OPE_B200_E_UNSUPPORTED, "FPN determination is not available in a batch");
     const float2* fpn = (c->cfg.fpn_removal && c->fpn.valid) ? c->fpn.d_profile : nullptr;
     *a = make_args(c, nullptr, nullptr, 0, fpn);
+    if (c->cfg.post_bg_removal) {
+        if (c->bg_record_requested)
+            return fail(c, OPE_B200_E_UNSUPPORTED, "post-process background recording is not available in a batch");
+        if (c->bg_valid) {
+            if (c->bgv_dirty) {
+                OPE_CU(c, bg_values(c->d_bg, c->n / 2, c->cfg.bg_weight, c->cfg.bg_offset, c->d_bgv, nullptr));
+                OPE_CU(c, cudaDeviceSynchronize());
+                c->bgv_dirty = false;
+            }
+            a->bgv = c->d_bgv;
+        }
+    }
     *n = c->n;
     *in_kind = c->in_kind;
     *interp = c->interp;
@@ -421,6 +438,8 @@ void ope_b200_destroy(ope_b200_ctx* c) {
     cudaFree(c->d_in);
     cudaFree(c->d_out);
     fpn_free(c->fpn);
+    cudaFree(c->d_bg);
+    cudaFree(c->d_bgv);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -441,6 +460,7 @@ int ope_b200_update_config(ope_b200_ctx* c, const ope_b200_config* cfg) {
         return fail(c, OPE_B200_E_STATE, "dimension change requires a new context");
     const bool dt_change = cfg->input_dtype != c->cfg.input_dtype || cfg->float32_as_uint32 != c->cfg.float32_as_uint32;
     c->cfg = *cfg;
+    c->bgv_dirty = true;  // background weight or offset may have changed
     if (dt_change) {
         c->in_kind = input_kind(cfg->input_dtype, cfg->float32_as_uint32 != 0);
         c->in_bytes = static_cast<size_t>(c->m) * c->n * bytes_of(cfg->input_dtype);
@@ -501,6 +521,26 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
     }
     ChainArgs a = make_args(c, d_in, bins ? nullptr : static_cast<float*>(d_out), m, fpn);
     if (bins) a.bins_out = static_cast<float2*>(d_out);
+    // post-process background (cpu_backend.cpp:283-301): a recording frame is
+    // scaled first, its mean A-scan becomes the profile, then it is subtracted;
+    // other frames subtract the profile in the chain epilogue
+    const int half = c->n / 2;
+    const bool bg_on = c->cfg.post_bg_removal && !bins;
+    const bool record = bg_on && c->bg_record_requested;
+    if (bg_on && (record || c->bg_valid)) {
+        if (!c->d_bg) OPE_CU(c, cudaMalloc(&c->d_bg, half * sizeof(float)));
+        if (!c->d_bgv) OPE_CU(c, cudaMalloc(&c->d_bgv, half * sizeof(float)));
+        // frames still in flight on other streams may read the current values:
+        // a recording or a changed weight/offset waits for them (rare events)
+        if (record || (c->bg_valid && c->bgv_dirty)) OPE_CU(c, cudaDeviceSynchronize());
+    }
+    if (bg_on && !record && c->bg_valid) {
+        if (c->bgv_dirty) {
+            OPE_CU(c, bg_values(c->d_bg, half, c->cfg.bg_weight, c->cfg.bg_offset, c->d_bgv, s));
+            c->bgv_dirty = false;
+        }
+        a.bgv = c->d_bgv;
+    }
     if (c->inject_stall_ns) {
         a.debug_skip_first_copy = 1;
         a.timeout_ns = c->inject_stall_ns;
@@ -509,6 +549,16 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
     cudaError_t e = launch_chain(c->n, c->in_kind, c->interp, a, s, 0, nullptr);
     if (e != cudaSuccess) return cuda_fail(c, e, "chain launch");
     OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
+    if (record) {
+        float* out = static_cast<float*>(d_out);
+        OPE_CU(c, bg_record(out, m, half, c->d_bg, s));
+        OPE_CU(c, bg_values(c->d_bg, half, c->cfg.bg_weight, c->cfg.bg_offset, c->d_bgv, s));
+        OPE_CU(c, bg_subtract(out, m, half, c->d_bgv, s));
+        c->bg_valid = true;
+        c->bgv_dirty = false;
+        c->bg_host_stale = true;
+        c->bg_record_requested = false;
+    }
     return OPE_B200_OK;
 }
 
@@ -551,7 +601,8 @@ int ope_b200_process_host(ope_b200_ctx* c, const void* h_in, float* h_out) {
     const long long B = c->cfg.bscans_per_buffer;
     const long long kChunks = 8;
     const long long bs_per_chunk = 2 * ((B + 2 * kChunks - 1) / (2 * kChunks));
-    const bool chunked = !(c->fpn.requested || c->cfg.fpn_continuous) && B >= 4;
+    const bool chunked = !(c->fpn.requested || c->cfg.fpn_continuous) &&
+                         !(c->cfg.post_bg_removal && c->bg_record_requested) && B >= 4;
     if (!chunked) {
         OPE_CU(c, cudaMemcpyAsync(c->d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, c->stream));
         int rc = process_locked(c, c->d_in, c->d_out, c->m, c->stream);
@@ -635,7 +686,7 @@ int ope_b200_request_bg_recording(ope_b200_ctx* c) {
     if (!c) return OPE_B200_E_INVALID;
     std::lock_guard<std::mutex> lk(c->mu);
     c->bg_record_requested = true;
-    return fail(c, OPE_B200_E_UNSUPPORTED, "post-process background recording is not implemented yet");
+    return OPE_B200_OK;
 }
 
 int ope_b200_set_bg_profile(ope_b200_ctx* c, const float* p, size_t n) {
@@ -646,12 +697,28 @@ int ope_b200_set_bg_profile(ope_b200_ctx* c, const float* p, size_t n) {
         return fail(c, OPE_B200_E_INVALID, "Invalid background buffer size. Expected " + std::to_string(c->n / 2) +
                                                " but got " + std::to_string(n));
     c->bg_profile.assign(p, p + n);
+    OPE_CU(c, cudaSetDevice(c->device));
+    if (!c->d_bg) OPE_CU(c, cudaMalloc(&c->d_bg, n * sizeof(float)));
+    if (!c->d_bgv) OPE_CU(c, cudaMalloc(&c->d_bgv, n * sizeof(float)));
+    OPE_CU(c, cudaDeviceSynchronize());  // no frame in flight still reads the old values
+    OPE_CU(c, cudaMemcpy(c->d_bg, p, n * sizeof(float), cudaMemcpyHostToDevice));
+    c->bg_valid = true;
+    c->bgv_dirty = true;
+    c->bg_host_stale = false;
     return OPE_B200_OK;
 }
 
 int ope_b200_get_bg_profile(ope_b200_ctx* c, float* out, size_t cap, size_t* n) {
     if (!c) return OPE_B200_E_INVALID;
     std::lock_guard<std::mutex> lk(c->mu);
+    if (c->bg_host_stale) {  // recorded on the device since the last read
+        OPE_CU(c, cudaSetDevice(c->device));
+        OPE_CU(c, cudaDeviceSynchronize());
+        c->bg_profile.resize(c->n / 2);
+        OPE_CU(c, cudaMemcpy(c->bg_profile.data(), c->d_bg, c->bg_profile.size() * sizeof(float),
+                             cudaMemcpyDeviceToHost));
+        c->bg_host_stale = false;
+    }
     if (n) *n = c->bg_profile.size();
     if (out) std::memcpy(out, c->bg_profile.data(), std::min(cap, c->bg_profile.size()) * sizeof(float));
     return OPE_B200_OK;

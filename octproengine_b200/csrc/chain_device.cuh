@@ -216,7 +216,8 @@ __device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, con
 #pragma unroll
         for (int q = 0; q < L::R / 2; ++q) {
             const int bin = L::bin(t, i, q);
-            const float2 r = res[i * (L::R / 2) + q];
+            float2 r = res[i * (L::R / 2) + q];
+            if (a.bgv) r = sub2(r, dup2(__ldg(a.bgv + bin)));
             __stcs(a.out + oa + bin, r.x);
             if (has_b) __stcs(a.out + ob + bin, r.y);
         }

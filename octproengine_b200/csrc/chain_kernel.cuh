@@ -79,6 +79,10 @@ struct ChainArgs {
     // is the same quantity computed with a far smaller float32 error floor.
     const float2* dc_resp;
     float* resampled_out;  // test hook (CPU emulation only): k-linearised spectrum of the last pair
+    // Post-process background (applyPostProcessBackgroundSubtraction,
+    // cpu_kernels.tpp:381-400): when set, bgv[b] = weight * profile[b] + offset
+    // is subtracted from every output value of bin b after the scaling.
+    const float* bgv;
 };
 
 template <int N_>

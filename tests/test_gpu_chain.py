@@ -230,3 +230,77 @@ def test_pipelined_process_host_matches_device_path(cuda, bscans, flip):
         ctx.close()
     b = H.gpu_run(spec, raw, fpn_profile=prof)
     assert np.array_equal(a, b)
+
+
+def _bg_spec(**kw):
+    return spec_for(2048, CUBIC, m=40).with_(grayscale_min=10.0, grayscale_max=90.0, **kw)
+
+
+def test_post_process_background_subtraction_is_exact(cuda):
+    # applyPostProcessBackgroundSubtraction (cpu_kernels.tpp:381-400):
+    # out - (weight * profile + offset), the last operation on each value
+    import ctypes
+    base = _bg_spec()
+    spec = base.with_()
+    raw = H.random_raw(spec, seed=31)
+    plain = H.gpu_run(base, raw)
+    prof = np.random.default_rng(5).uniform(0.0, 0.5, 1024).astype(np.float32)
+    cfg = spec.to_config()
+    cfg.post_bg_removal = 1
+    cfg.bg_weight = 0.75
+    cfg.bg_offset = -0.125
+    ctx = capi.Context(cfg)
+    r, w, cs = spec.curves()
+    ctx.set_resampling_curve(r)
+    ctx.set_window_curve(w)
+    ctx.set_dispersion_curve(cs)
+    try:
+        capi._check(ctx.h, capi.lib().ope_b200_set_bg_profile(ctx.h, capi.fptr(prof), prof.size))
+        got = H.gpu_run(spec, raw, ctx=ctx)
+    finally:
+        ctx.close()
+    bgv = (np.float32(0.75) * prof + np.float32(-0.125)).astype(np.float32)
+    assert np.array_equal(got, (plain - bgv[None, :]).astype(np.float32))
+    st = R.ChainSettings(n=2048, resampling=True, interpolation=CUBIC, windowing=True, dispersion=True,
+                         grayscale_min=10.0, grayscale_max=90.0, ascans_per_bscan=40, post_bg_removal=True,
+                         bg_weight=0.75, bg_offset=-0.125)
+    ref = R.process_buffer(raw, st, R.Curves(r, w, cs[0::2].copy(), cs[1::2].copy()), bg_profile=prof).output
+    assert np.abs(got - ref).max() * 80.0 < 1e-2
+
+
+def test_post_process_background_recording(cuda):
+    # recordPostProcessBackground (cpu_backend.cpp:105-118): float sum over the
+    # frame's A-scans in order, divided by their count; then subtracted from
+    # the same frame (cpu_backend.cpp:283-301)
+    import ctypes
+    spec = _bg_spec()
+    raw = H.random_raw(spec, seed=32)
+    plain = H.gpu_run(spec, raw)
+    acc = np.zeros(1024, np.float32)
+    for row in plain:
+        acc = (acc + row).astype(np.float32)
+    want_prof = (acc / np.float32(plain.shape[0])).astype(np.float32)
+    cfg = spec.to_config()
+    cfg.post_bg_removal = 1
+    cfg.bg_weight = 1.0
+    cfg.bg_offset = 0.0
+    ctx = capi.Context(cfg)
+    r, w, cs = spec.curves()
+    ctx.set_resampling_curve(r)
+    ctx.set_window_curve(w)
+    ctx.set_dispersion_curve(cs)
+    try:
+        capi._check(ctx.h, capi.lib().ope_b200_request_bg_recording(ctx.h))
+        first = H.gpu_run(spec, raw, ctx=ctx)
+        prof = np.zeros(1024, np.float32)
+        n = ctypes.c_size_t(0)
+        capi._check(ctx.h, capi.lib().ope_b200_get_bg_profile(ctx.h, capi.fptr(prof), 1024, ctypes.byref(n)))
+        raw2 = H.random_raw(spec, seed=33)
+        second = H.gpu_run(spec, raw2, ctx=ctx)  # subtracts the recorded profile
+        assert ctx.synchronize() == 0
+    finally:
+        ctx.close()
+    assert n.value == 1024 and np.array_equal(prof, want_prof)
+    assert np.array_equal(first, (plain - want_prof[None, :]).astype(np.float32))
+    plain2 = H.gpu_run(spec, raw2)
+    assert np.array_equal(second, (plain2 - want_prof[None, :]).astype(np.float32))
