@@ -130,10 +130,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from octproengine_b200.multirank import rank_setup
+    return rank_setup()
 
 
 def cpu_reference_run(steps: int, warmup: int, threads: int, bscans_per_thread: int = 1):
@@ -404,15 +402,13 @@ def run_ours(args):
         ev1.record(stream)
         barrier()
         time.sleep(0.25)
+    from octproengine_b200.multirank import max_over_ranks, weak_scaling_rate
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, device=dev)  # the slowest rank's device time
     if ctx.synchronize() != 0:
         raise RuntimeError("chain kernel reported a device status")
     ms_step = ms_max / args.steps
-    value = world * M / (ms_step / 1e3)
+    value = weak_scaling_rate(M, ms_step / 1e3, world)
 
     # kernel-only launch duration (the one chain kernel per step)
     kernel_ms = ms / args.steps
@@ -473,11 +469,8 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         ctx.process_host(raw_np, out_np)
-    e2e_dt = time.perf_counter() - t0
-    tt = torch.tensor([e2e_dt], device=dev)
-    if dist is not None:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = world * M * e2e_steps / float(tt.item())
+    e2e_dt = max_over_ranks(time.perf_counter() - t0, device=dev)
+    e2e_value = weak_scaling_rate(M * e2e_steps, e2e_dt, world)
 
     autofocus = None
     if world == 1 and not args.no_autofocus:
