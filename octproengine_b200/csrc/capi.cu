@@ -102,6 +102,11 @@ struct ope_b200_ctx {
     float* d_bgv = nullptr;  // weight * profile + offset, n/2
     bool bg_valid = false, bgv_dirty = true, bg_host_stale = false;
 
+    // sinusoidal scan correction: curve (A-scans per B-scan) and scratch image
+    float* d_sin_curve = nullptr;
+    float* d_sin_tmp = nullptr;
+    size_t sin_tmp_bytes = 0;
+
     // host-path buffers
     void* d_in = nullptr;
     float* d_out = nullptr;
@@ -308,6 +313,8 @@ int ctx_batch_args(ope_b200_ctx* c, ChainArgs* a, int* n, int* in_kind, int* int
     }
     if (c->fpn.requested || c->cfg.fpn_continuous)
         return fail(c, OPE_B200_E_UNSUPPORTED, "FPN determination is not available in a batch");
+    if (c->cfg.sinusoidal_correction)
+        return fail(c, OPE_B200_E_UNSUPPORTED, "sinusoidal scan correction is not available in a batch");
     const float2* fpn = (c->cfg.fpn_removal && c->fpn.valid) ? c->fpn.d_profile : nullptr;
     *a = make_args(c, nullptr, nullptr, 0, fpn);
     if (c->cfg.post_bg_removal) {
@@ -440,6 +447,8 @@ void ope_b200_destroy(ope_b200_ctx* c) {
     fpn_free(c->fpn);
     cudaFree(c->d_bg);
     cudaFree(c->d_bgv);
+    cudaFree(c->d_sin_curve);
+    cudaFree(c->d_sin_tmp);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -534,12 +543,32 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
         // a recording or a changed weight/offset waits for them (rare events)
         if (record || (c->bg_valid && c->bgv_dirty)) OPE_CU(c, cudaDeviceSynchronize());
     }
-    if (bg_on && !record && c->bg_valid) {
-        if (c->bgv_dirty) {
-            OPE_CU(c, bg_values(c->d_bg, half, c->cfg.bg_weight, c->cfg.bg_offset, c->d_bgv, s));
-            c->bgv_dirty = false;
+    if (bg_on && !record && c->bg_valid && c->bgv_dirty) {
+        OPE_CU(c, bg_values(c->d_bg, half, c->cfg.bg_weight, c->cfg.bg_offset, c->d_bgv, s));
+        c->bgv_dirty = false;
+    }
+    const float* bgv_now = (bg_on && !record && c->bg_valid) ? c->d_bgv : nullptr;
+    // sinusoidal scan correction (cuda_backend.cu:696-706, after the flip and
+    // before the background): the chain writes a scratch image, the correction
+    // interpolates across A-scans into the output and subtracts the background
+    const bool sin_on = c->cfg.sinusoidal_correction && !bins;
+    if (sin_on) {
+        const size_t need = static_cast<size_t>(m) * half * sizeof(float);
+        if (need > c->sin_tmp_bytes) {
+            OPE_CU(c, cudaStreamSynchronize(s));
+            cudaFree(c->d_sin_tmp);
+            c->d_sin_tmp = nullptr;
+            c->sin_tmp_bytes = 0;
+            OPE_CU(c, cudaMalloc(&c->d_sin_tmp, need));
+            c->sin_tmp_bytes = need;
         }
-        a.bgv = c->d_bgv;
+        if (!c->d_sin_curve) {
+            OPE_CU(c, cudaMalloc(&c->d_sin_curve, c->cfg.ascans_per_bscan * sizeof(float)));
+            OPE_CU(c, sin_curve(c->d_sin_curve, c->cfg.ascans_per_bscan, s));
+        }
+        a.out = c->d_sin_tmp;
+    } else {
+        a.bgv = bgv_now;
     }
     if (c->inject_stall_ns) {
         a.debug_skip_first_copy = 1;
@@ -549,6 +578,9 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
     cudaError_t e = launch_chain(c->n, c->in_kind, c->interp, a, s, 0, nullptr);
     if (e != cudaSuccess) return cuda_fail(c, e, "chain launch");
     OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
+    if (sin_on)
+        OPE_CU(c, sin_correct(static_cast<float*>(d_out), c->d_sin_tmp, c->d_sin_curve, half,
+                              c->cfg.ascans_per_bscan, m, bgv_now, s));
     if (record) {
         float* out = static_cast<float*>(d_out);
         OPE_CU(c, bg_record(out, m, half, c->d_bg, s));
@@ -602,7 +634,8 @@ int ope_b200_process_host(ope_b200_ctx* c, const void* h_in, float* h_out) {
     const long long kChunks = 8;
     const long long bs_per_chunk = 2 * ((B + 2 * kChunks - 1) / (2 * kChunks));
     const bool chunked = !(c->fpn.requested || c->cfg.fpn_continuous) &&
-                         !(c->cfg.post_bg_removal && c->bg_record_requested) && B >= 4;
+                         !(c->cfg.post_bg_removal && c->bg_record_requested) && !c->cfg.sinusoidal_correction &&
+                         B >= 4;
     if (!chunked) {
         OPE_CU(c, cudaMemcpyAsync(c->d_in, h_in, c->in_bytes, cudaMemcpyHostToDevice, c->stream));
         int rc = process_locked(c, c->d_in, c->d_out, c->m, c->stream);

@@ -514,3 +514,44 @@ def process_buffer(raw, st: ChainSettings, curves: Curves, mode: str = "ref",
         res.spectrum = z
         res.ifft = X
     return res
+
+
+# --------------------------------------------------------------------------
+# sinusoidal scan correction: the reference CUDA backend only
+# (cuda_kernels.cu:408-438, applied at cuda_backend.cu:696-706); the CPU
+# backend has no such step, so this restates the CUDA kernels.
+# --------------------------------------------------------------------------
+
+def sinusoidal_curve(length: int) -> np.ndarray:
+    """fillSinusoidalScanCorrectionCurve: (L/pi) acos(1 - 2k/L), float acos."""
+    k = np.arange(length, dtype=np.float64)
+    arg = (1.0 - (2.0 * k.astype(F32).astype(np.float64)) / float(F32(length))).astype(F32)
+    ac = np.arccos(arg).astype(F32).astype(np.float64)
+    return ((float(F32(length)) / math.pi) * ac).astype(F32)
+
+
+def sinusoidal_correction(img: np.ndarray, ascans_per_bscan: int, curve: Optional[np.ndarray] = None) -> np.ndarray:
+    """sinusoidalScanCorrection on a (A-scans, bins) float32 image: A-scan k of
+    each B-scan interpolates between input A-scans (int)x and (int)x + 1 of the
+    same flat buffer (x = curve[k]); the last A-scan of the buffer is kept. The
+    interpolation is one fused multiply-add (f1 - f0) * frac + f0, rounded once
+    (evaluated exactly in float64)."""
+    m, width = img.shape
+    h = ascans_per_bscan
+    if curve is None:
+        curve = sinusoidal_curve(h)
+    flat = img.reshape(-1).astype(F32)
+    out = flat.copy()
+    idx = np.arange(m * width - width, dtype=np.int64)
+    j = idx % width
+    k = (idx // width) % h
+    l = idx // (width * h)
+    x = curve[k].astype(F32)
+    xi = x.astype(np.int32).astype(np.int64)
+    x0 = xi * width + j + l * width * h
+    f0 = flat[x0]
+    f1 = flat[x0 + width]
+    frac = (x - xi.astype(F32)).astype(F32)
+    d = (f1 - f0).astype(F32)
+    out[idx] = (d.astype(np.float64) * frac.astype(np.float64) + f0.astype(np.float64)).astype(F32)
+    return out.reshape(m, width)

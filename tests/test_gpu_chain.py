@@ -304,3 +304,39 @@ def test_post_process_background_recording(cuda):
     assert np.array_equal(first, (plain - want_prof[None, :]).astype(np.float32))
     plain2 = H.gpu_run(spec, raw2)
     assert np.array_equal(second, (plain2 - want_prof[None, :]).astype(np.float32))
+
+
+@pytest.mark.parametrize("with_bg", [False, True])
+def test_sinusoidal_scan_correction(cuda, with_bg):
+    # sinusoidalScanCorrection of the reference CUDA backend (cuda_kernels.cu:
+    # 408-438): lateral resampling after the flip, before the background
+    spec = spec_for(1024, CUBIC, m=64).with_(bscans_per_buffer=3, bscan_flip=True)
+    raw = H.random_raw(spec, seed=41)
+    plain = H.gpu_run(spec, raw)
+    cfg = spec.to_config()
+    cfg.sinusoidal_correction = 1
+    prof = np.random.default_rng(9).uniform(0, 0.3, 512).astype(np.float32)
+    if with_bg:
+        cfg.post_bg_removal = 1
+        cfg.bg_weight = 2.0
+        cfg.bg_offset = 0.25
+    ctx = capi.Context(cfg)
+    r, w, cs = spec.curves()
+    ctx.set_resampling_curve(r)
+    ctx.set_window_curve(w)
+    ctx.set_dispersion_curve(cs)
+    try:
+        if with_bg:
+            capi._check(ctx.h, capi.lib().ope_b200_set_bg_profile(ctx.h, capi.fptr(prof), prof.size))
+        got = H.gpu_run(spec, raw, ctx=ctx)
+        assert ctx.synchronize() == 0
+    finally:
+        ctx.close()
+    want = R.sinusoidal_correction(plain, 64)
+    if with_bg:
+        want = (want - (np.float32(2.0) * prof + np.float32(0.25))[None, :]).astype(np.float32)
+    assert np.array_equal(got[-1], want[-1])  # last A-scan passes through
+    # the curve comes from the device acosf, the restatement from numpy's: a
+    # last-bit difference in x (ulp up to 4e-6 for x < 64) moves the fraction,
+    # so outputs agree to |f1 - f0| * 4e-6 rather than to the last bit
+    assert np.allclose(got, want, rtol=0, atol=1e-5), np.abs(got - want).max()
