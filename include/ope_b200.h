@@ -282,6 +282,59 @@ OPE_B200_API int ope_b200_batch_get_tuning(ope_b200_batch* batch, int32_t n, int
  * events, best kept) and keeps the fastest. Overwrites the outputs. */
 OPE_B200_API int ope_b200_batch_autotune(ope_b200_batch* batch, int32_t reps);
 
+/* ---- low-level per-operation API: the unit-level operations of
+ *      ProcessingBackend (backend_interface.h:50-164, Processor
+ *      include/processor.h:165-282), each one GPU kernel on HOST arrays,
+ *      synchronous (copy in, kernel, copy out). Where the reference CPU backend
+ *      implements the operation (cpu_backend.cpp:514-733) the arithmetic is its
+ *      kernels' (cpu_kernels.tpp); its CUDA backend returns empty results for
+ *      all of them (cuda_backend.cu:1133-1296). All outputs are float arrays. ---- */
+/* convertInput: samples of bit depth <= 8 / <= 16 / else read as uint8 / uint16 /
+ * uint32 and converted to float (cpu_kernels.tpp:24-54; the bitshift flag is not
+ * applied, as in the CPU backend). */
+OPE_B200_API int ope_b200_op_convert_input(const void* input, int32_t bit_depth, int64_t samples, float* out);
+/* kLinearization of one line (method: ope::InterpolationMethod); the first
+ * `samples` outputs (cpu_backend.cpp:533-570). */
+OPE_B200_API int ope_b200_op_klinearization(const float* input, const float* curve, int32_t method,
+                                            int32_t line_width, int64_t samples, float* out);
+/* mode 1: windowing (cpu_backend.cpp:572-597); 2: dispersionCompensation, real
+ * part, phase as 2*line_width interleaved (cos, sin) (:599-627); 3: dispersion
+ * then window (dispersionCompensationAndWindowing). First `samples` outputs. */
+OPE_B200_API int ope_b200_op_window_dispersion(const float* input, const float* window, const float* phase_cos_sin,
+                                               int32_t mode, int32_t line_width, int64_t samples, float* out);
+/* |DFT| of one real line, all line_width outputs: inverse = 1 is the reference's
+ * ifft (unnormalised exp(+i), cpu_backend.cpp:634-659), 0 the forward transform;
+ * evaluated in double. */
+OPE_B200_API int ope_b200_op_dft_magnitude(const float* input, int32_t line_width, int32_t inverse, float* out);
+/* getMinimumVarianceMean over height rows of width interleaved complex values:
+ * 2*width floats (cpu_kernels.tpp:402-458, same double accumulation). */
+OPE_B200_API int ope_b200_op_min_variance_mean(const float* input, int32_t width, int32_t height, int32_t segments,
+                                               float* out);
+/* fixedPatternNoiseRemoval (cpu_backend.cpp:701-733): mean line subtracted as the
+ * reference's meanALineSubtraction does on the flattened buffer, then |z|. */
+OPE_B200_API int ope_b200_op_fpn_removal(const float* input, const float* mean_line, int32_t line_width,
+                                         int32_t num_lines, float* out);
+/* rollingAverageBackgroundRemoval per line, the reference kernel's float running
+ * sum (cpu_kernels.tpp:56-82). */
+OPE_B200_API int ope_b200_op_rolling_dc_removal(const float* input, int32_t window, int32_t line_width,
+                                                int32_t num_lines, float* out);
+/* bscanFlip with the chain's rule (even B-scans that have a successor mirrored). */
+OPE_B200_API int ope_b200_op_bscan_flip(const float* input, int32_t line_width, int32_t lines_per_bscan,
+                                        int32_t num_bscans, float* out);
+/* sinusoidalScanCorrection with the given curve (lines_per_bscan floats; NULL =
+ * the reference's curve), cuda_kernels.cu:408-438 semantics. */
+OPE_B200_API int ope_b200_op_sinusoidal_correction(const float* input, const float* curve, int32_t line_width,
+                                                   int32_t lines_per_bscan, int32_t num_bscans, float* out);
+/* postProcessTruncate: log or linear scaling of lines of line_width interleaved
+ * complex values to line_width/2 outputs each (cpu_kernels.tpp:301-378, auto
+ * range per line when min == max in log mode). */
+OPE_B200_API int ope_b200_op_truncate(const float* input, int32_t log_scaling, float grayscale_max,
+                                      float grayscale_min, float addend, float multiplicator, int32_t line_width,
+                                      int64_t num_lines, float* out);
+/* postProcessBackgroundSubtraction: in[i] - (weight * bg[i % line_width] + offset). */
+OPE_B200_API int ope_b200_op_background_subtraction(const float* input, const float* background_line, float weight,
+                                                    float offset, int32_t line_width, int64_t samples, float* out);
+
 /* Test hook, no reference counterpart: the next launch of this context skips
  * its first input copy, so its bounded wait runs out after `timeout_us`; the
  * kernel then records a status that ope_b200_synchronize / process_host

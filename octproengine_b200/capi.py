@@ -130,6 +130,21 @@ SIGNATURES = {
     "ope_b200_batch_get_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]),
     "ope_b200_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "ope_b200_op_convert_input": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int64, _FP]),
+    "ope_b200_op_klinearization": (ctypes.c_int, [_FP, _FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _FP]),
+    "ope_b200_op_window_dispersion": (ctypes.c_int, [_FP, _FP, _FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64,
+                                                     _FP]),
+    "ope_b200_op_dft_magnitude": (ctypes.c_int, [_FP, ctypes.c_int32, ctypes.c_int32, _FP]),
+    "ope_b200_op_min_variance_mean": (ctypes.c_int, [_FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _FP]),
+    "ope_b200_op_fpn_removal": (ctypes.c_int, [_FP, _FP, ctypes.c_int32, ctypes.c_int32, _FP]),
+    "ope_b200_op_rolling_dc_removal": (ctypes.c_int, [_FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _FP]),
+    "ope_b200_op_bscan_flip": (ctypes.c_int, [_FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _FP]),
+    "ope_b200_op_sinusoidal_correction": (ctypes.c_int, [_FP, _FP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                         _FP]),
+    "ope_b200_op_truncate": (ctypes.c_int, [_FP, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_float, ctypes.c_int32, ctypes.c_int64, _FP]),
+    "ope_b200_op_background_subtraction": (ctypes.c_int, [_FP, _FP, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                                          ctypes.c_int64, _FP]),
     "ope_b200_abi_version": (ctypes.c_int, []),
     "ope_b200_device_supported": (ctypes.c_int, [ctypes.c_int32]),
 }

@@ -306,40 +306,138 @@ const std::vector<float>& B200Backend::getFixedPatternNoiseProfile() const {
     return m.fpn_profile;
 }
 
-// Low-level per-operation test API (processor.h:165-282). The reference CUDA
-// backend returns empty results for all of them (cuda_backend.cu:1133-1296);
-// this backend does the same.
-std::vector<float> B200Backend::convertInput(const void*, IOBuffer::DataType, int, int, bool) { return {}; }
-std::vector<float> B200Backend::rollingAverageBackgroundRemoval(const float*, int, int, int) { return {}; }
-std::vector<float> B200Backend::kLinearization(const float*, const float*, InterpolationMethod, int, int) {
-    return {};
+// Low-level per-operation API (processor.h:165-282): each operation is one
+// GPU kernel of the C ABI (ope_b200_op_*, octproengine_b200/csrc/ops.cu) on
+// host arrays. The reference CPU backend implements convertInput,
+// kLinearization, windowing, dispersionCompensation, ifft,
+// getMinimumVarianceMean and fixedPatternNoiseRemoval and returns zero vectors
+// for the others; the reference CUDA backend returns empty vectors for all.
+namespace {
+
+std::vector<float> op_result(int rc, std::vector<float>&& out, const char* what) {
+    if (rc != OPE_B200_OK) throw std::runtime_error(std::string(what) + ": low-level operation failed");
+    return std::move(out);
 }
-std::vector<float> B200Backend::windowing(const float*, const float*, int, int) { return {}; }
-std::vector<float> B200Backend::dispersionCompensation(const float*, const float*, int, int) { return {}; }
-std::vector<float> B200Backend::kLinearizationAndWindowing(const float*, const float*, const float*,
-                                                           InterpolationMethod, int, int) {
-    return {};
+
+}  // namespace
+
+std::vector<float> B200Backend::convertInput(const void* input, IOBuffer::DataType, int bitDepth, int samples,
+                                             bool) {
+    std::vector<float> out(samples > 0 ? samples : 0);
+    if (!input || samples <= 0) return out;
+    return op_result(ope_b200_op_convert_input(input, bitDepth, samples, out.data()), std::move(out), "convertInput");
 }
-std::vector<float> B200Backend::kLinearizationAndWindowingAndDispersion(const float*, const float*, const float*,
-                                                                        const float*, InterpolationMethod, int,
-                                                                        int) {
-    return {};
+
+std::vector<float> B200Backend::rollingAverageBackgroundRemoval(const float* input, int windowSize, int lineWidth,
+                                                                int numLines) {
+    std::vector<float> out(static_cast<size_t>(lineWidth) * numLines);
+    return op_result(ope_b200_op_rolling_dc_removal(input, windowSize, lineWidth, numLines, out.data()),
+                     std::move(out), "rollingAverageBackgroundRemoval");
 }
-std::vector<float> B200Backend::dispersionCompensationAndWindowing(const float*, const float*, const float*, int,
-                                                                   int) {
-    return {};
+
+std::vector<float> B200Backend::kLinearization(const float* input, const float* resampleCurve,
+                                               InterpolationMethod method, int lineWidth, int samples) {
+    std::vector<float> out(samples);
+    return op_result(ope_b200_op_klinearization(input, resampleCurve, static_cast<int>(method), lineWidth, samples,
+                                                out.data()),
+                     std::move(out), "kLinearization");
 }
-std::vector<float> B200Backend::fft(const float*, int, int) { return {}; }
-std::vector<float> B200Backend::ifft(const float*, int, int) { return {}; }
-std::vector<float> B200Backend::getMinimumVarianceMean(const float*, int, int, int) { return {}; }
-std::vector<float> B200Backend::fixedPatternNoiseRemoval(const float*, const float*, int, int) { return {}; }
-std::vector<float> B200Backend::postProcessTruncate(const float*, bool, float, float, float, float, int, int) {
-    return {};
+
+std::vector<float> B200Backend::windowing(const float* input, const float* windowCurve, int lineWidth, int samples) {
+    std::vector<float> out(samples);
+    return op_result(ope_b200_op_window_dispersion(input, windowCurve, nullptr, 1, lineWidth, samples, out.data()),
+                     std::move(out), "windowing");
 }
-std::vector<float> B200Backend::bscanFlip(const float*, int, int, int) { return {}; }
-std::vector<float> B200Backend::sinusoidalScanCorrection(const float*, const float*, int, int, int) { return {}; }
-std::vector<float> B200Backend::postProcessBackgroundSubtraction(const float*, const float*, float, float, int, int) {
-    return {};
+
+std::vector<float> B200Backend::dispersionCompensation(const float* input, const float* phaseComplex, int lineWidth,
+                                                       int samples) {
+    std::vector<float> out(samples);
+    return op_result(ope_b200_op_window_dispersion(input, nullptr, phaseComplex, 2, lineWidth, samples, out.data()),
+                     std::move(out), "dispersionCompensation");
+}
+
+std::vector<float> B200Backend::kLinearizationAndWindowing(const float* input, const float* resampleCurve,
+                                                           const float* windowCurve, InterpolationMethod method,
+                                                           int lineWidth, int samples) {
+    std::vector<float> k = kLinearization(input, resampleCurve, method, lineWidth, lineWidth);
+    return windowing(k.data(), windowCurve, lineWidth, samples);
+}
+
+std::vector<float> B200Backend::kLinearizationAndWindowingAndDispersion(const float* input, const float* resampleCurve,
+                                                                        const float* windowCurve,
+                                                                        const float* phaseComplex,
+                                                                        InterpolationMethod method, int lineWidth,
+                                                                        int samples) {
+    std::vector<float> k = kLinearizationAndWindowing(input, resampleCurve, windowCurve, method, lineWidth, lineWidth);
+    return dispersionCompensation(k.data(), phaseComplex, lineWidth, samples);
+}
+
+std::vector<float> B200Backend::dispersionCompensationAndWindowing(const float* input, const float* phaseComplex,
+                                                                   const float* windowCurve, int lineWidth,
+                                                                   int samples) {
+    std::vector<float> out(samples);
+    return op_result(ope_b200_op_window_dispersion(input, windowCurve, phaseComplex, 3, lineWidth, samples,
+                                                   out.data()),
+                     std::move(out), "dispersionCompensationAndWindowing");
+}
+
+std::vector<float> B200Backend::fft(const float* input, int lineWidth, int) {
+    std::vector<float> out(lineWidth);
+    return op_result(ope_b200_op_dft_magnitude(input, lineWidth, 0, out.data()), std::move(out), "fft");
+}
+
+std::vector<float> B200Backend::ifft(const float* input, int lineWidth, int) {
+    std::vector<float> out(lineWidth);
+    return op_result(ope_b200_op_dft_magnitude(input, lineWidth, 1, out.data()), std::move(out), "ifft");
+}
+
+std::vector<float> B200Backend::getMinimumVarianceMean(const float* input, int width, int height, int segments) {
+    if (!input) return {};
+    std::vector<float> out(static_cast<size_t>(width) * 2);
+    return op_result(ope_b200_op_min_variance_mean(input, width, height, segments, out.data()), std::move(out),
+                     "getMinimumVarianceMean");
+}
+
+std::vector<float> B200Backend::fixedPatternNoiseRemoval(const float* input, const float* meanALine, int lineWidth,
+                                                         int numLines) {
+    if (!input) return {};
+    std::vector<float> out(static_cast<size_t>(lineWidth) * numLines);
+    return op_result(ope_b200_op_fpn_removal(input, meanALine, lineWidth, numLines, out.data()), std::move(out),
+                     "fixedPatternNoiseRemoval");
+}
+
+std::vector<float> B200Backend::postProcessTruncate(const float* input, bool logScaling, float grayscaleMax,
+                                                    float grayscaleMin, float addend, float multiplicator,
+                                                    int lineWidth, int samples) {
+    const long long lines = lineWidth > 1 ? (2LL * samples) / lineWidth : 0;
+    std::vector<float> out(static_cast<size_t>(lines) * (lineWidth / 2));
+    if (lines == 0) return out;
+    return op_result(ope_b200_op_truncate(input, logScaling ? 1 : 0, grayscaleMax, grayscaleMin, addend, multiplicator,
+                                          lineWidth, lines, out.data()),
+                     std::move(out), "postProcessTruncate");
+}
+
+std::vector<float> B200Backend::bscanFlip(const float* input, int lineWidth, int linesPerBscan, int numBscans) {
+    std::vector<float> out(static_cast<size_t>(lineWidth) * linesPerBscan * numBscans);
+    return op_result(ope_b200_op_bscan_flip(input, lineWidth, linesPerBscan, numBscans, out.data()), std::move(out),
+                     "bscanFlip");
+}
+
+std::vector<float> B200Backend::sinusoidalScanCorrection(const float* input, const float* resampleCurve,
+                                                         int lineWidth, int linesPerBscan, int numBscans) {
+    std::vector<float> out(static_cast<size_t>(lineWidth) * linesPerBscan * numBscans);
+    return op_result(ope_b200_op_sinusoidal_correction(input, resampleCurve, lineWidth, linesPerBscan, numBscans,
+                                                       out.data()),
+                     std::move(out), "sinusoidalScanCorrection");
+}
+
+std::vector<float> B200Backend::postProcessBackgroundSubtraction(const float* input, const float* backgroundLine,
+                                                                 float weight, float offset, int lineWidth,
+                                                                 int samples) {
+    std::vector<float> out(samples);
+    return op_result(ope_b200_op_background_subtraction(input, backgroundLine, weight, offset, lineWidth, samples,
+                                                        out.data()),
+                     std::move(out), "postProcessBackgroundSubtraction");
 }
 
 }  // namespace ope
