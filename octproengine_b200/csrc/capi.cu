@@ -113,7 +113,7 @@ struct ope_b200_ctx {
 
     // pipelined host path (ope_b200_process_host)
     cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
-    cudaEvent_t ev_pipe[16] = {};
+    cudaEvent_t ev_pipe[128] = {};
 
     // test hook: next launch skips its first bulk copy and waits at most this long
     unsigned long long inject_stall_ns = 0;
@@ -631,7 +631,9 @@ int ope_b200_process_host(ope_b200_ctx* c, const void* h_in, float* h_out) {
     // parities; FPN determination needs the whole buffer and runs unchunked.
     const long long A = c->cfg.ascans_per_bscan;
     const long long B = c->cfg.bscans_per_buffer;
-    const long long kChunks = 8;
+    // 16 chunks: measured 6.28 ms per 2048 x 1024 x 64 uint16 buffer (4: 6.88,
+    // 8: 6.36, 32: 6.52) against 5.64 ms for the bare concurrent copies
+    const long long kChunks = 16;
     const long long bs_per_chunk = 2 * ((B + 2 * kChunks - 1) / (2 * kChunks));
     const bool chunked = !(c->fpn.requested || c->cfg.fpn_continuous) &&
                          !(c->cfg.post_bg_removal && c->bg_record_requested) && !c->cfg.sinusoidal_correction &&
