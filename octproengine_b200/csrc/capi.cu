@@ -106,6 +106,8 @@ struct ope_b200_ctx {
     float* d_sin_curve = nullptr;
     float* d_sin_tmp = nullptr;
     size_t sin_tmp_bytes = 0;
+    cudaEvent_t ev_sin = nullptr;  // last use of the scratch image (frames on other streams wait for it)
+    bool ev_sin_recorded = false;
 
     // host-path buffers
     void* d_in = nullptr;
@@ -449,6 +451,7 @@ void ope_b200_destroy(ope_b200_ctx* c) {
     cudaFree(c->d_bgv);
     cudaFree(c->d_sin_curve);
     cudaFree(c->d_sin_tmp);
+    if (c->ev_sin) cudaEventDestroy(c->ev_sin);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -566,6 +569,10 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
             OPE_CU(c, cudaMalloc(&c->d_sin_curve, c->cfg.ascans_per_bscan * sizeof(float)));
             OPE_CU(c, sin_curve(c->d_sin_curve, c->cfg.ascans_per_bscan, s));
         }
+        if (!c->ev_sin) OPE_CU(c, cudaEventCreateWithFlags(&c->ev_sin, cudaEventDisableTiming));
+        // one scratch image per context: a frame on another stream (the ring)
+        // must have finished its correction before this chain overwrites it
+        if (c->ev_sin_recorded) OPE_CU(c, cudaStreamWaitEvent(s, c->ev_sin, 0));
         a.out = c->d_sin_tmp;
     } else {
         a.bgv = bgv_now;
@@ -578,9 +585,12 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
     cudaError_t e = launch_chain(c->n, c->in_kind, c->interp, a, s, 0, nullptr);
     if (e != cudaSuccess) return cuda_fail(c, e, "chain launch");
     OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
-    if (sin_on)
+    if (sin_on) {
         OPE_CU(c, sin_correct(static_cast<float*>(d_out), c->d_sin_tmp, c->d_sin_curve, half,
                               c->cfg.ascans_per_bscan, m, bgv_now, s));
+        OPE_CU(c, cudaEventRecord(c->ev_sin, s));
+        c->ev_sin_recorded = true;
+    }
     if (record) {
         float* out = static_cast<float*>(d_out);
         OPE_CU(c, bg_record(out, m, half, c->d_bg, s));

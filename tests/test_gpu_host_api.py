@@ -280,3 +280,49 @@ def test_cpp_processor_stream(cuda, tmp_path):
     want = _reference_outputs(spec, frames)
     for g, w in zip(got, want):
         np.testing.assert_array_equal(g, w)
+
+
+def test_ring_with_sinusoidal_correction_and_background(cuda):
+    # the sinusoidal scratch image is shared by the context: frames that overlap
+    # on the ring's streams must still come out as one-at-a-time processing
+    import torch
+    spec = _spec(n=1024, a=64, b=2)
+    cfg = spec.to_config()
+    cfg.sinusoidal_correction = 1
+    cfg.post_bg_removal = 1
+    cfg.bg_weight = 0.5
+    cfg.bg_offset = 0.1
+    frames = _frames(spec, 6, seed=60)
+    prof = np.linspace(0.0, 0.2, 512, dtype=np.float32)
+
+    def make():
+        ctx = capi.Context(cfg)
+        r, w, cs = spec.curves()
+        ctx.set_resampling_curve(r)
+        ctx.set_window_curve(w)
+        ctx.set_dispersion_curve(cs)
+        capi._check(ctx.h, capi.lib().ope_b200_set_bg_profile(ctx.h, capi.fptr(prof), prof.size))
+        return ctx
+
+    ref = make()
+    try:
+        want = [ref.process_host(f).copy() for f in frames]
+    finally:
+        ref.close()
+    ctx = make()
+    try:
+        pinned = [torch.from_numpy(f.view(np.uint8).reshape(-1).copy()).pin_memory() for f in frames]
+        depth = capi.lib().ope_b200_ring_depth(ctx.h)
+        tickets = [ctx.submit(pinned[k].data_ptr()) for k in range(depth)]
+        nxt, done = depth, 0
+        while done < len(frames):
+            out = ctx.wait(tickets[done], 20000)
+            np.testing.assert_array_equal(out, want[done])
+            ctx.release(tickets[done])
+            done += 1
+            if nxt < len(frames):
+                tickets.append(ctx.submit(pinned[nxt].data_ptr()))
+                nxt += 1
+        assert ctx.synchronize() == 0
+    finally:
+        ctx.close()
