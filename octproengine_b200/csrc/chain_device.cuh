@@ -288,7 +288,22 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
 
         // ---- unpack (+ DC removal or exact DC split) ----
         float2 dc = make_float2(0.0f, 0.0f);
-        if (a.dc_window > 0) {
+        // 8/16-bit samples without rolling-average DC removal: packed integer
+        // spectrum (bit-identical taps, half the shared-memory bytes)
+        constexpr bool PACKABLE = (DT == IN_U8 || DT == IN_U16);
+        const bool packed = PACKABLE && a.dc_window == 0;
+        float2 cbias = dup2(8388608.0f);
+        if (packed) {
+            uint32_t words[16];
+            int sa, sb;
+            phase_split_load_packed<N, DT>(t, stage, words, &sa, &sb);
+            if (a.dc_resp) {
+                team_sum2<T, int>(tm, sa, sb, reinterpret_cast<int*>(scan));
+                dc = make_float2(split_level((double)sa, N, true), split_level((double)sb, N, true));
+                cbias = add2(cbias, dc);  // 2^23 + c, exact for c < 2^23
+            }
+            phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
+        } else if (a.dc_window > 0) {
             sum_t ta, tb;
             phase_dc_local<N, DT>(t, stage, &ta, &tb);
             team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan);
@@ -311,7 +326,8 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
 
         // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];
-        phase_prestage<N, INTERP>(t, spec, a, v);
+        if (packed) phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v);
+        else phase_prestage<N, INTERP>(t, spec, a, v);
         fft_twiddle_dft<N, 0, false, S>(t, v, a.tw);
         tm.sync();  // spec aliases the exchange buffer
         fft_store<N, 0, S>(t, v, exch);

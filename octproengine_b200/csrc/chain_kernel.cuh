@@ -341,6 +341,85 @@ OPE_HD void phase_split_store(int t, const float2* vals, float2 c, float2* spec)
     }
 }
 
+// ------------------------------------------ packed integer spectrum (8/16-bit) --
+// For 8- and 16-bit samples without rolling-average DC removal the unpacked
+// spectrum is kept as integers: one 32-bit word per sample holds the pair's
+// two raw samples (row a in the low half, row b in the high half), half the
+// bytes of the float pair. A tap is converted in registers exactly:
+// (2^23 + u) - (2^23 + c) = u - c, the same float as the float spectrum holds.
+
+OPE_HD float2 packed_to_pair(uint32_t w, float2 cbias) {
+#if defined(__CUDA_ARCH__)
+    const float lo = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5410));
+    const float hi = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5432));
+#else
+    const float lo = bits_f(static_cast<int>(0x4B000000u | (w & 0xFFFFu)));
+    const float hi = bits_f(static_cast<int>(0x4B000000u | (w >> 16)));
+#endif
+    return sub2(make_float2(lo, hi), cbias);
+}
+
+// Samples 2p and 2p+1 of both rows as packed words; adds them to the row sums.
+template <int DT>
+OPE_HD void load_pos2_packed(const unsigned char* stage, int n, int p, uint32_t* w, int* sa, int* sb) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    const raw_t* ra = reinterpret_cast<const raw_t*>(stage);
+    const raw_t* rb = ra + n;
+    uint32_t a0, a1, b0, b1;
+#if defined(__CUDA_ARCH__)
+    if (DT == IN_U16) {
+        const uint32_t wa = *reinterpret_cast<const uint32_t*>(ra + 2 * p);
+        const uint32_t wb = *reinterpret_cast<const uint32_t*>(rb + 2 * p);
+        w[0] = __byte_perm(wa, wb, 0x5410);
+        w[1] = __byte_perm(wa, wb, 0x7632);
+        *sa += (int)(wa & 0xFFFFu) + (int)(wa >> 16);
+        *sb += (int)(wb & 0xFFFFu) + (int)(wb >> 16);
+        return;
+    }
+#endif
+    a0 = ra[2 * p];
+    a1 = ra[2 * p + 1];
+    b0 = rb[2 * p];
+    b1 = rb[2 * p + 1];
+    w[0] = a0 | (b0 << 16);
+    w[1] = a1 | (b1 << 16);
+    *sa += (int)(a0 + a1);
+    *sb += (int)(b0 + b1);
+}
+
+// Step A of the packed path: thread t packs the sample pairs p = t + k*T
+// (k < 8) and sums each row (exact integers).
+template <int N, int DT>
+OPE_HD void phase_split_load_packed(int t, const unsigned char* stage, uint32_t* words, int* sa, int* sb) {
+    constexpr int T = Plan<N>::T;
+    int a = 0, b = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) load_pos2_packed<DT>(stage, N, t + k * T, words + 2 * k, &a, &b);
+    *sa = a;
+    *sb = b;
+}
+
+// Step C of the packed path: the words into the spectrum with replicated edges.
+template <int N>
+OPE_HD void phase_store_packed(int t, const uint32_t* words, uint32_t* specw) {
+    constexpr int T = Plan<N>::T;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int p = t + k * T;
+        OPE_SMEM_CHECK(SPEC_PAD + 2 * p + 1 < N + 2 * SPEC_PAD);
+#if defined(__CUDA_ARCH__)
+        *reinterpret_cast<uint2*>(&specw[SPEC_PAD + 2 * p]) = make_uint2(words[2 * k], words[2 * k + 1]);
+#else
+        specw[SPEC_PAD + 2 * p] = words[2 * k];
+        specw[SPEC_PAD + 2 * p + 1] = words[2 * k + 1];
+#endif
+        if (p == 0)
+            for (int e = 0; e < SPEC_PAD; ++e) specw[e] = words[0];
+        if (p == N / 2 - 1)
+            for (int e = 0; e < SPEC_PAD; ++e) specw[SPEC_PAD + N + e] = words[2 * k + 1];
+    }
+}
+
 // Rolling-average DC removal (cpu_kernels.tpp:56-82): x[i] -= mean of
 // x[i-(W-1) .. min(i+W, N-1)]. Window sums come from exact integer prefix sums
 // (the reference accumulates them in float; for integer input whose running
@@ -485,6 +564,70 @@ OPE_HD void phase_prestage(int t, const float2* spec, const ChainArgs& a, cp* v)
         // re = y*w*cos, im = y*w*sin with the window folded into the phase
         // factors (w*cos, w*sin), evaluated in double and rounded once and
         // shared by both lanes.
+#if defined(__CUDA_ARCH__)
+        const float2 q = __ldg(a.wph + j);
+#else
+        const float2 q = a.wph[j];
+#endif
+        v[s] = cpmake(mul2x(y, dup2(q.x), NZ), mul2x(y, dup2(q.y), NZ));
+    }
+}
+
+// phase_prestage on the packed integer spectrum: the same interpolation and
+// window-phase arithmetic on the same (exactly converted) tap values.
+template <int N, int INTERP>
+OPE_HD void phase_prestage_packed(int t, const uint32_t* specw, float2 cbias, const ChainArgs& a, cp* v) {
+    constexpr int T = Plan<N>::T;
+    const float2 NZ = dup2(a.neg_zero);
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+        const int j = t + s * T;
+        float2 y;
+        if (INTERP == INTERP_NONE) {
+            y = packed_to_pair(specw[SPEC_PAD + j], cbias);
+        } else if (INTERP == INTERP_LINEAR) {
+#if defined(__CUDA_ARCH__)
+            const int2 e = __ldg(a.lin + j);
+#else
+            const int2 e = a.lin[j];
+#endif
+            OPE_SMEM_CHECK(e.x >= 0 && e.x + 1 < N + 2 * SPEC_PAD);
+            const float2 y1 = packed_to_pair(specw[e.x], cbias);
+            const float2 y2 = packed_to_pair(specw[e.x + 1], cbias);
+            y = add2(y1, mul2x(sub2(y2, y1), dup2(bits_f(e.y)), NZ));
+        } else if (INTERP == INTERP_CUBIC) {
+#if defined(__CUDA_ARCH__)
+            const int2 e = __ldg(a.cub + j);
+#else
+            const int2 e = a.cub[j];
+#endif
+            const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
+            OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 + 2 < N + 2 * SPEC_PAD);
+            const float pos = bits_f(e.y), pos2 = fmul_rn(pos, pos);
+            const float2 y0 = packed_to_pair(specw[i0], cbias), y1 = packed_to_pair(specw[i1], cbias);
+            const float2 y2 = packed_to_pair(specw[i1 + 1], cbias), y3 = packed_to_pair(specw[i1 + 2], cbias);
+            float2 ca = add2(sub2(mul2x(dup2(3.0f), sub2(y1, y2), NZ), y0), y3);
+            float2 cb = sub2(add2(sub2(mul2x(dup2(2.0f), y0, NZ), mul2x(dup2(5.0f), y1, NZ)),
+                                  mul2x(dup2(4.0f), y2, NZ)),
+                             y3);
+            float2 cc = sub2(y2, y0);
+            float2 in = add2(add2(mul2x(ca, dup2(pos2), NZ), mul2x(cb, dup2(pos), NZ)), cc);
+            y = add2(mul2x(dup2(fmul_rn(0.5f, pos)), in, NZ), y1);
+        } else {
+            const int b = a.lz_base[j];
+            OPE_SMEM_CHECK(b >= 0 && b + 15 < N + 2 * SPEC_PAD);
+            float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+#if defined(__CUDA_ARCH__)
+                const float w = __ldg(a.lz_w + k * N + j);
+#else
+                const float w = a.lz_w[k * N + j];
+#endif
+                acc = add2(acc, mul2x(packed_to_pair(specw[b + k], cbias), dup2(w), NZ));
+            }
+            y = acc;
+        }
 #if defined(__CUDA_ARCH__)
         const float2 q = __ldg(a.wph + j);
 #else
