@@ -176,22 +176,69 @@ def cpu_reference_run(steps: int, warmup: int, threads: int, bscans_per_thread: 
     return ascans / dt, dt, ascans
 
 
+def cuda_reference_run(steps: int, warmup: int, interp=None):
+    """Times the reference CUDA backend (oracle/_ref/libope_cuda_ref.so: the
+    reference's cuda_backend.cu + cuda_kernels.cu, cuFFT for the DFT, built with
+    the reference's default flags) on the benchmark workload through its own
+    API: each step is one process() of a 64-B-scan buffer from the backend's
+    registered input ring (2 buffers, the reference default), H2D + kernels +
+    D2H, counted at its output callback. Its first frame determines the FPN
+    profile (warm-up); timed frames subtract it."""
+    from oracle import refcuda
+    from octproengine_b200 import synth
+    spec = bench_spec(interp)
+    if not refcuda.available():
+        refcuda.build()
+    p = refcuda.make_params(N, ASCANS, BSCANS, 2, resampling=True, interpolation=spec.interpolation,
+                            resampling_coeffs=spec.resampling_coeffs, windowing=True, window_type=spec.window_type,
+                            window_center=spec.window_center, window_fill=spec.window_fill, dispersion=True,
+                            dispersion_coeffs=spec.dispersion_coeffs, fpn_removal=True,
+                            grayscale_min=spec.grayscale_min, grayscale_max=spec.grayscale_max)
+    raw = synth.as_numpy(synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=BSCANS, seed=100,
+                                                          background_ripple=True)), "uint16")
+    be = refcuda.RefCudaBackend(p)
+    try:
+        be.fill_inputs(raw)
+        be.stream(warmup)
+        dt = be.stream(steps)
+    finally:
+        be.close()
+    m = ASCANS * BSCANS
+    return {"value": steps * m / dt, "unit": UNIT, "ms_per_step": 1e3 * dt / steps,
+            "h2d_bytes_per_step": m * N * 2, "d2h_bytes_per_step": m * (N // 2) * 4}
+
+
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    rate, dt, ascans = cpu_reference_run(args.steps, args.warmup, threads)
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "impl": "reference", "metric": METRIC, "value": None, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": f"{threads} x 1 B-scan (1024 A-scans) per step"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{ascans} A-scans: {threads} reference CpuBackend instances in parallel, "
-                                   f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW"},
-        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_cpu_baseline:
+        rate, dt, ascans = cpu_reference_run(args.steps, args.warmup, threads)
+        line.update({
+            "value": rate, "ms_per_step": 1e3 * dt / args.steps,
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{ascans} A-scans: {threads} reference CpuBackend instances in parallel, "
+                                       f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        })
+    if not args.no_cuda_reference:
+        # the reference's own GPU path on the same workload, end to end through its API
+        from octproengine_b200.chain import LANCZOS
+        try:
+            cb = cuda_reference_run(args.steps, args.warmup)
+            cb["variants"] = {"lanczos8": cuda_reference_run(max(3, args.steps // 2), args.warmup, LANCZOS)}
+            cb["kind"] = ("reference CudaBackend (cuda_backend.cu + cuda_kernels.cu, cuFFT), --use_fast_math, "
+                          "sm_100; end to end: registered host ring, H2D + chain + D2H per buffer")
+            line["cuda_backend"] = cb
+        except Exception as e:  # no GPU, or the library could not be built here
+            line["cuda_backend"] = {"unavailable": str(e).splitlines()[0][:200]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -526,6 +573,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cuda-reference", action="store_true",
+                    help="reference arm: skip timing the reference CUDA backend")
     ap.add_argument("--no-autofocus", action="store_true", help="skip the autofocus fit-versus-sweep line")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-buffer line")
     ap.add_argument("--bscans", type=int, default=BSCANS, help="B-scans per buffer (profiling uses fewer)")

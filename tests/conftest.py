@@ -39,6 +39,20 @@ def reflib():
 
 
 @pytest.fixture(scope="session")
+def refcuda():
+    """The reference CUDA backend built out of tree (oracle/_ref), a comparison baseline."""
+    from oracle import refcuda as R
+    if not R.available():
+        try:
+            R.build()
+        except Exception as e:  # pragma: no cover - depends on the machine
+            pytest.skip(f"reference CUDA backend not buildable here: {e}")
+    if not R.available():
+        pytest.skip("reference CUDA backend library not present")
+    return R
+
+
+@pytest.fixture(scope="session")
 def cuda():
     import torch
     if not torch.cuda.is_available():
