@@ -391,6 +391,131 @@ def batch_bench(dev, seed=3, count=32, steps=20):
             "per_length": per_len, "gpu_launches_per_batch": 1}
 
 
+def ring_stream(ctx, inputs, frames: int, fit=None) -> float:
+    """Pushes `frames` buffers (cycling over the pinned host tensors `inputs`)
+    back to back through the context's frame ring (submit / wait / release,
+    as many in flight as the ring has slots); each frame's output lands in the
+    slot's pinned host buffer. `fit(k)`, when given, runs on the host while
+    frames are in flight, before frame k is waited for. Returns wall seconds
+    from the first submit to the last completed frame."""
+    from collections import deque
+    depth = ctx_ring_depth(ctx)
+    tickets = deque()
+    k = done = 0
+    t0 = time.perf_counter()
+    while done < frames:
+        while k < frames and len(tickets) < depth:
+            tickets.append(ctx.submit(inputs[k % len(inputs)].data_ptr()))
+            k += 1
+        if fit is not None:
+            fit(done)
+        t = tickets.popleft()
+        ctx.wait(t, 60000)
+        ctx.release(t)
+        done += 1
+    return time.perf_counter() - t0
+
+
+def ctx_ring_depth(ctx) -> int:
+    from octproengine_b200 import capi
+    return int(capi.lib().ope_b200_ring_depth(ctx.h))
+
+
+def streaming_bench(dev, chunks=16, bscans_per_chunk=32, pool=4, n=4096, ascans=1024, seed=5):
+    """The streaming-volume workload: 4096 samples x 1024 A-scans x 512 B-scans
+    uint16 (4 GiB raw) pushed from pinned host memory through the frame ring in
+    32-B-scan chunks (cubic resampling, Hann window, dispersion compensation,
+    float32 log output, the chunk's output back in pinned host memory), with a
+    gradient dispersion fit (Lanczos-8, entropy) of one B-scan per chunk on a
+    separate stream, overlapped with the ring. The host holds `pool` distinct
+    chunks (seeded synthetic scenes sharing one hidden dispersion) and cycles
+    over them, as a frame grabber cycles over its buffers. Fit error = max over
+    (d2, d3) of |fit - true| / max(|true|, 1 rad) against the generating
+    dispersion."""
+    import torch
+    from octproengine_b200 import capi, synth
+    from octproengine_b200.chain import ChainSpec, open_context, CUBIC, HANN
+    from octproengine_b200.autofocus import Autofocus, fit_dispersion, dispersion_poly, LANCZOS
+    rng = np.random.default_rng(seed)
+    d2, d3 = float(rng.uniform(-40, 40)), float(rng.uniform(-20, 20))
+    s = 2048.0 / n  # the k-map's non-linearity scaled to the record length
+    kc = (synth.K_COEFFS[0], synth.K_COEFFS[1], synth.K_COEFFS[2] * s, synth.K_COEFFS[3] * s * s)
+    ctrue = synth.linearising_coeffs(n, kc)
+    m = ascans * bscans_per_chunk
+    spec = ChainSpec(signal_length=n, ascans_per_bscan=ascans, bscans_per_buffer=bscans_per_chunk,
+                     resampling=True, interpolation=CUBIC, resampling_coeffs=ctrue, windowing=True,
+                     window_type=HANN, window_center=0.5, window_fill=0.95, dispersion=True,
+                     dispersion_coeffs=tuple(dispersion_poly(d2, d3)), grayscale_min=20.0, grayscale_max=100.0,
+                     device=dev.index or 0)
+    pinned = []
+    x = None
+    for p in range(pool):
+        x = synth.generate(synth.SynthParams(n=n, ascans=ascans, bscans=bscans_per_chunk, seed=300 + p, d2=d2,
+                                             d3=d3, resampling_truth=ctrue), device=dev)
+        h = torch.empty(x.numel() * 2, dtype=torch.uint8).pin_memory()
+        h.copy_(x.view(torch.uint8).reshape(-1).cpu())
+        pinned.append(h)
+    # device-resident chain on one chunk (kernel only)
+    out = torch.empty((m, n // 2), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ctx = open_context(spec)
+    for _ in range(3):
+        ctx.process_device(x.data_ptr(), out.data_ptr(), stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        ctx.process_device(x.data_ptr(), out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    kms = e0.elapsed_time(e1) / 10
+    del x, out
+    ctx.close()
+    peak, _ = measured_peak()
+    res = {"workload": (f"{n} samples x {ascans} A-scans x {chunks * bscans_per_chunk} B-scans uint16 "
+                        f"({chunks * m * n * 2 / 2**30:.0f} GiB raw) in {bscans_per_chunk}-B-scan chunks through the "
+                        f"frame ring from pinned host memory ({pool} distinct chunks cycled), cubic, Hann, "
+                        f"dispersion, float32 log output to pinned host; fit: one {ascans}-A-scan B-scan per "
+                        f"chunk, Lanczos-8 entropy, on its own stream"),
+           "unit": "A-scans/s", "hidden_d2": d2, "hidden_d3": d3,
+           "device_resident_chunk": {"value": m / (kms / 1e3), "ms_per_chunk": kms,
+                                     "hbm_frac": m * algorithmic_bytes_per_ascan(n) / (kms / 1e3) / 1e9 / peak}}
+    window = capi.generate_window_curve(n, HANN, 0.5, 0.95)
+    af = Autofocus(n, "uint16", LANCZOS, window=window, device=dev.index or 0)
+    fit_stream = torch.cuda.Stream(dev)
+    fitbuf = torch.empty((ascans, n), dtype=torch.int16, device=dev)
+    fits = []
+
+    def fit(k):
+        with torch.cuda.stream(fit_stream):
+            fitbuf.view(torch.uint8).reshape(-1).copy_(pinned[k % pool][:ascans * n * 2], non_blocking=True)
+            fits.append(fit_dispersion(af, fitbuf, ctrue))
+
+    def err(f):
+        return max(abs(f.d2 - d2) / max(abs(d2), 1.0), abs(f.d3 - d3) / max(abs(d3), 1.0))
+
+    for depth in (2, 3):
+        ctx = open_context(spec.with_(num_input_buffers=depth))
+        ring_stream(ctx, pinned, 2)  # slots, pinned outputs, first launches
+        dt = ring_stream(ctx, pinned, chunks)
+        res[f"ring_depth{depth}"] = {"value": chunks * m / dt, "seconds": dt,
+                                     "host_gbs": chunks * m * (n * 2 + n // 2 * 4) / dt / 1e9}
+        if depth == 2:
+            fit(0)  # graph capture paths and the fit's first launches
+            fits.clear()
+            torch.cuda.synchronize(dev)
+            dt = ring_stream(ctx, pinned, chunks, fit=fit)
+            torch.cuda.synchronize(dev)
+            errs = [err(f) for f in fits]
+            res["with_fits"] = {"value": chunks * m / dt, "seconds": dt, "fits": len(fits),
+                                "fit_seconds_median": float(np.median([f.seconds for f in fits])),
+                                "fit_error_median": float(np.median(errs)), "fit_error_max": float(max(errs)),
+                                "fits_within_1pct": int(sum(e < 0.01 for e in errs))}
+        ctx.close()
+    af.close()
+    res["value"] = res["with_fits"]["value"]
+    return res
+
+
 def run_ours(args):
     import torch
     from octproengine_b200 import synth
@@ -519,12 +644,27 @@ def run_ours(args):
     e2e_dt = max_over_ranks(time.perf_counter() - t0, device=dev)
     e2e_value = weak_scaling_rate(M * e2e_steps, e2e_dt, world)
 
+    # sustained end to end through the frame ring (frames back to back, as the
+    # reference's ring is driven): depth 2, the reference's default
+    ctx_r = open_context(spec.with_(num_input_buffers=2))
+    ctx_r.set_fpn_profile(ctx.fpn_profile())
+    ring_in = [xh.view(torch.uint8).reshape(-1)]
+    ring_stream(ctx_r, ring_in, 2)
+    barrier()
+    ring_dt = max_over_ranks(ring_stream(ctx_r, ring_in, e2e_steps), device=dev)
+    ctx_r.close()
+    e2e_stream = {"value": weak_scaling_rate(M * e2e_steps, ring_dt, world), "unit": UNIT,
+                  "ring_depth": 2, "h2d_bytes_per_step": M * N * 2, "d2h_bytes_per_step": M * (N // 2) * 4}
+
     autofocus = None
     if world == 1 and not args.no_autofocus:
         autofocus = autofocus_bench(dev)
     batched = None
     if world == 1 and not args.no_batch:
         batched = batch_bench(dev)
+    streaming = None
+    if world == 1 and not args.no_streaming:
+        streaming = streaming_bench(dev)
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -551,6 +691,7 @@ def run_ours(args):
                      "algorithmic_bytes": bytes_launch},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 2,
                 "d2h_bytes_per_step": M * (N // 2) * 4},
+        "e2e_stream": e2e_stream,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "variants": variants,
@@ -559,6 +700,8 @@ def run_ours(args):
         line["autofocus"] = autofocus
     if batched:
         line["batched"] = batched
+    if streaming:
+        line["streaming_volume"] = streaming
     if cpu_base:
         line["cpu_baseline"] = cpu_base
     print(json.dumps(line), flush=True)
@@ -577,6 +720,7 @@ def main():
                     help="reference arm: skip timing the reference CUDA backend")
     ap.add_argument("--no-autofocus", action="store_true", help="skip the autofocus fit-versus-sweep line")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-buffer line")
+    ap.add_argument("--no-streaming", action="store_true", help="skip the streaming-volume line")
     ap.add_argument("--bscans", type=int, default=BSCANS, help="B-scans per buffer (profiling uses fewer)")
     ap.add_argument("--interp", default="cubic", choices=["linear", "cubic", "lanczos"])
     ap.add_argument("--kernel-only", action="store_true",

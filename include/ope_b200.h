@@ -238,6 +238,13 @@ OPE_B200_API int ope_b200_af_forward(ope_b200_af* af, const void* d_in, int64_t 
 OPE_B200_API int ope_b200_af_backward(ope_b200_af* af, const void* d_in, int64_t num_ascans, const float* d_params,
                                       int32_t output_mode, const float* d_grad_out, const double* d_hs,
                                       float* d_grad_params, void* stream);
+/* 1 when kernels can use `ptr` at that address (device memory, or page-locked
+ * host memory under unified addressing), else 0. */
+OPE_B200_API int ope_b200_af_kernel_accessible(const void* ptr);
+/* Copies `bytes` (<= 4096) on `stream` with one small kernel instead of a
+ * copy-engine DMA; both pointers must be kernel-accessible. For a fit's
+ * parameters and results, which otherwise wait behind bulk frame copies. */
+OPE_B200_API int ope_b200_af_small_copy(void* dst, const void* src, int32_t bytes, void* stream);
 
 /* ---- batched chain: many buffers of uneven geometry in ONE persistent launch.
  *      No counterpart in the reference, whose backends process one IOBuffer of

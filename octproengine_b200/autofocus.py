@@ -195,7 +195,10 @@ class _Evaluator:
     With ``graph`` the whole evaluation (parameter upload from pinned host
     memory, forward, adjoint, result download) is captured once in a CUDA
     graph and replayed, so an evaluation costs one graph launch and one
-    synchronisation on the host.
+    synchronisation on the host. The 80 bytes of parameters and results move
+    by a small kernel (ope_b200_af_small_copy) rather than by copy-engine DMA,
+    so an evaluation does not wait behind bulk transfers that other streams
+    have queued on the copy engines (frames streaming through a ring).
     """
 
     def __init__(self, af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], graph: bool = True):
@@ -210,6 +213,9 @@ class _Evaluator:
         self.h_grad = torch.empty(8, dtype=torch.float32, pin_memory=True)
         self.count = 0
         self.graph = None
+        L = capi.lib()
+        self.sm_copies = all(L.ope_b200_af_kernel_accessible(_ptr(t)) == 1 for t in
+                             (self.h_params, self.d_params, self.h_hs, self.d_hs, self.h_grad, self.d_grad))
         self._set(np.zeros(2))
         if graph:
             side = torch.cuda.Stream(dev)
@@ -227,12 +233,21 @@ class _Evaluator:
         hp[:4] = dispersion_poly(theta[0], theta[1])
         hp[4:] = self.kmap
 
+    def _copy(self, dst: torch.Tensor, src: torch.Tensor, stream) -> None:
+        if not self.sm_copies:
+            dst.copy_(src, non_blocking=True)
+            return
+        rc = capi.lib().ope_b200_af_small_copy(_ptr(dst), _ptr(src), src.numel() * src.element_size(),
+                                               _stream(stream))
+        if rc != capi.OK:
+            raise capi.B200Error(rc, "small copy failed")
+
     def _enqueue(self, stream) -> None:
-        self.d_params.copy_(self.h_params, non_blocking=True)
+        self._copy(self.d_params, self.h_params, stream)
         self.af.forward(self.raw, self.d_params, hs=self.d_hs, stream=stream)
         self.af.backward(self.raw, self.d_params, self.d_grad, hs=self.d_hs, stream=stream)
-        self.h_hs.copy_(self.d_hs, non_blocking=True)
-        self.h_grad.copy_(self.d_grad, non_blocking=True)
+        self._copy(self.h_hs, self.d_hs, stream)
+        self._copy(self.h_grad, self.d_grad, stream)
 
     def __call__(self, theta: np.ndarray):
         self._set(theta)

@@ -55,6 +55,7 @@ class ChainSpec:
     float32_as_uint32: bool = False
     dc_split: bool = True
     device: int = 0
+    num_input_buffers: int = 2  # depth of the host frame ring
     # custom curves (used instead of the generated ones when given)
     resampling_curve: Optional[np.ndarray] = field(default=None, repr=False)
     window_curve: Optional[np.ndarray] = field(default=None, repr=False)
@@ -95,6 +96,7 @@ class ChainSpec:
         c.float32_as_uint32 = int(self.float32_as_uint32)
         c.dc_split = int(self.dc_split)
         c.device = int(self.device)
+        c.num_input_buffers = int(self.num_input_buffers)
         return c
 
     # curves as the reference Processor hands them to its backend

@@ -237,6 +237,16 @@ int af_prepare(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float
 
 }  // namespace
 
+// A few bytes moved by one warp pair's loads and stores. Between page-locked
+// host memory and the device this crosses the link as ordinary memory traffic,
+// so it does not queue behind bulk copies waiting on the copy engines (a fit's
+// parameter upload and result download while frames stream in and out).
+constexpr int AF_SMALL_COPY_MAX = 4096;
+
+__global__ void af_small_copy_kernel(unsigned char* dst, const unsigned char* src, int bytes) {
+    for (int i = threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
+}
+
 extern "C" {
 
 int ope_b200_af_create(int32_t n, int32_t input_dtype, int32_t interpolation, const float* window, int32_t device,
@@ -346,6 +356,26 @@ int ope_b200_af_backward(ope_b200_af* o, const void* d_in, int64_t num_ascans, c
     af_grad_finalize<<<1, 256, 0, s>>>(o->partial, grid, d_grad_params);
     AF_CU(o, cudaGetLastError());
     return OPE_B200_OK;
+}
+
+int ope_b200_af_kernel_accessible(const void* ptr) {
+    if (!ptr) return 0;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return 1;
+    // page-locked host memory: usable in kernels at the same address (unified addressing)
+    return at.type == cudaMemoryTypeHost && at.devicePointer == ptr ? 1 : 0;
+}
+
+int ope_b200_af_small_copy(void* dst, const void* src, int32_t bytes, void* stream) {
+    if (!dst || !src || bytes < 0 || bytes > AF_SMALL_COPY_MAX) return OPE_B200_E_INVALID;
+    if (bytes == 0) return OPE_B200_OK;
+    af_small_copy_kernel<<<1, 64, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src), bytes);
+    return cudaGetLastError() == cudaSuccess ? OPE_B200_OK : OPE_B200_E_CUDA;
 }
 
 }  // extern "C"

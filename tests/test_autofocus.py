@@ -211,3 +211,28 @@ def test_rejects_bad_arguments(cuda):
         af.forward(raw, d_p)  # neither an image nor (H, S) requested
     with pytest.raises(TypeError):
         af.forward(raw.float(), d_p, hs=torch.empty(2, dtype=torch.float64, device=cuda))
+
+
+def test_small_copies_move_fit_parameters_without_copy_engines(cuda):
+    import ctypes
+    import torch
+    from octproengine_b200 import capi
+    L = capi.lib()
+    h = torch.arange(20, dtype=torch.float32).pin_memory()
+    d = torch.zeros(20, dtype=torch.float32, device=cuda)
+    back = torch.zeros(20, dtype=torch.float32).pin_memory()
+    pageable = np.zeros(20, np.float32)
+    assert L.ope_b200_af_kernel_accessible(ctypes.c_void_p(h.data_ptr())) == 1
+    assert L.ope_b200_af_kernel_accessible(ctypes.c_void_p(d.data_ptr())) == 1
+    assert L.ope_b200_af_kernel_accessible(ctypes.c_void_p(pageable.ctypes.data)) == 0
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.ope_b200_af_small_copy(ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(h.data_ptr()), 80, s) == capi.OK
+    assert L.ope_b200_af_small_copy(ctypes.c_void_p(back.data_ptr() + 4), ctypes.c_void_p(d.data_ptr()), 75,
+                                    s) == capi.OK  # unaligned destination, odd size
+    torch.cuda.synchronize()
+    assert torch.equal(d.cpu(), h)
+    want = np.zeros(20, np.float32).view(np.uint8)
+    want[4:79] = h.numpy().view(np.uint8)[:75]
+    assert np.array_equal(back.numpy().view(np.uint8), want)
+    assert L.ope_b200_af_small_copy(ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(h.data_ptr()), 5000,
+                                    s) == capi.E_INVALID
