@@ -213,6 +213,7 @@ def test_rejects_bad_arguments(cuda):
         af.forward(raw.float(), d_p, hs=torch.empty(2, dtype=torch.float64, device=cuda))
 
 
+@pytest.mark.gpu
 def test_small_copies_move_fit_parameters_without_copy_engines(cuda):
     import ctypes
     import torch
