@@ -189,6 +189,23 @@ def test_fit_recovers_hidden_dispersion(cuda):
 
 
 @pytest.mark.gpu
+def test_reused_evaluator_serves_new_data_like_a_fresh_one(cuda):
+    from octproengine_b200.autofocus import FitEvaluator, fit_dispersion
+    cases = [make_case(m=128, seed=s, d2=d2, d3=d3) for s, d2, d3 in ((21, 15.0, -8.0), (22, -25.0, 6.0))]
+    window, ctrue = cases[0][2], cases[0][3]
+    af = _af(cuda, O.LANCZOS, window)
+    buf = cases[0][0].to(cuda)
+    ev = FitEvaluator(af, buf, ctrue)
+    for raw_t, _, _, _ in cases:
+        buf.copy_(raw_t.to(cuda))  # new data in the evaluator's tensor
+        reused = fit_dispersion(af, buf, ctrue, evaluator=ev)
+        fresh = fit_dispersion(af, raw_t.to(cuda), ctrue)
+        assert (reused.d2, reused.d3, reused.evaluations) == (fresh.d2, fresh.d3, fresh.evaluations)
+    with pytest.raises(ValueError):
+        fit_dispersion(af, cases[0][0].to(cuda), ctrue, evaluator=ev)  # another tensor
+
+
+@pytest.mark.gpu
 def test_grid_sweep_finds_the_nearest_grid_point(cuda):
     from octproengine_b200.autofocus import grid_sweep
     d2, d3 = 13.0, -6.5
