@@ -395,9 +395,9 @@ def ring_stream(ctx, inputs, frames: int, fit=None) -> float:
     """Pushes `frames` buffers (cycling over the pinned host tensors `inputs`)
     back to back through the context's frame ring (submit / wait / release,
     as many in flight as the ring has slots); each frame's output lands in the
-    slot's pinned host buffer. `fit(k)`, when given, runs on the host while
-    frames are in flight, before frame k is waited for. Returns wall seconds
-    from the first submit to the last completed frame."""
+    slot's pinned host buffer. `fit(k, ticket)`, when given, runs on the host
+    while frames are in flight, before frame k is waited for. Returns wall
+    seconds from the first submit to the last completed frame."""
     from collections import deque
     depth = ctx_ring_depth(ctx)
     tickets = deque()
@@ -408,7 +408,7 @@ def ring_stream(ctx, inputs, frames: int, fit=None) -> float:
             tickets.append(ctx.submit(inputs[k % len(inputs)].data_ptr()))
             k += 1
         if fit is not None:
-            fit(done)
+            fit(done, tickets[0])
         t = tickets.popleft()
         ctx.wait(t, 60000)
         ctx.release(t)
@@ -435,7 +435,8 @@ def streaming_bench(dev, chunks=16, bscans_per_chunk=32, pool=4, n=4096, ascans=
     import torch
     from octproengine_b200 import capi, synth
     from octproengine_b200.chain import ChainSpec, open_context, CUBIC, HANN
-    from octproengine_b200.autofocus import Autofocus, FitEvaluator, fit_dispersion, dispersion_poly, LANCZOS
+    from octproengine_b200.autofocus import Autofocus, FitEvaluator, fit_dispersion, dispersion_poly, \
+        frame_input_view, LANCZOS
     rng = np.random.default_rng(seed)
     d2, d3 = float(rng.uniform(-40, 40)), float(rng.uniform(-20, 20))
     s = 2048.0 / n  # the k-map's non-linearity scaled to the record length
@@ -475,23 +476,25 @@ def streaming_bench(dev, chunks=16, bscans_per_chunk=32, pool=4, n=4096, ascans=
                         f"({chunks * m * n * 2 / 2**30:.0f} GiB raw) in {bscans_per_chunk}-B-scan chunks through the "
                         f"frame ring from pinned host memory ({pool} distinct chunks cycled), cubic, Hann, "
                         f"dispersion, float32 log output to pinned host; fit: one {ascans}-A-scan B-scan per "
-                        f"chunk, Lanczos-8 entropy, on its own stream"),
+                        f"chunk read in place from the ring slot, Lanczos-8 entropy, on its own stream"),
            "unit": "A-scans/s", "hidden_d2": d2, "hidden_d3": d3,
            "device_resident_chunk": {"value": m / (kms / 1e3), "ms_per_chunk": kms,
                                      "hbm_frac": m * algorithmic_bytes_per_ascan(n) / (kms / 1e3) / 1e9 / peak}}
     window = capi.generate_window_curve(n, HANN, 0.5, 0.95)
     af = Autofocus(n, "uint16", LANCZOS, window=window, device=dev.index or 0)
     fit_stream = torch.cuda.Stream(dev)
-    fitbuf = torch.empty((ascans, n), dtype=torch.int16, device=dev)
-    fitbuf.view(torch.uint8).reshape(-1).copy_(pinned[0][:ascans * n * 2])
-    with torch.cuda.stream(fit_stream):
-        ev = FitEvaluator(af, fitbuf, ctrue)  # one graph, reused by every chunk's fit
     fits = []
+    evaluators = {}  # per ring slot: a view of its device input and one captured fit graph
 
-    def fit(k):
+    def fit(k, ticket):
+        # the chunk's first B-scan, read in place from the ring slot's device copy
         with torch.cuda.stream(fit_stream):
-            fitbuf.view(torch.uint8).reshape(-1).copy_(pinned[k % pool][:ascans * n * 2], non_blocking=True)
-            fits.append(fit_dispersion(af, fitbuf, ctrue, evaluator=ev))
+            view = frame_input_view(ctx, ticket, ascans, fit_stream)
+            key = view.data_ptr()
+            if key not in evaluators:
+                evaluators[key] = (view, FitEvaluator(af, view, ctrue))
+            view, ev = evaluators[key]
+            fits.append(fit_dispersion(af, view, ctrue, evaluator=ev))
 
     def err(f):
         return max(abs(f.d2 - d2) / max(abs(d2), 1.0), abs(f.d3 - d3) / max(abs(d3), 1.0))
@@ -503,7 +506,7 @@ def streaming_bench(dev, chunks=16, bscans_per_chunk=32, pool=4, n=4096, ascans=
         res[f"ring_depth{depth}"] = {"value": chunks * m / dt, "seconds": dt,
                                      "host_gbs": chunks * m * (n * 2 + n // 2 * 4) / dt / 1e9}
         if depth == 2:
-            fit(0)  # graph capture paths and the fit's first launches
+            ring_stream(ctx, pinned, depth, fit=fit)  # one fit graph per ring slot, captured here
             fits.clear()
             torch.cuda.synchronize(dev)
             dt = ring_stream(ctx, pinned, chunks, fit=fit)

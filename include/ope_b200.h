@@ -149,6 +149,12 @@ OPE_B200_API int ope_b200_submit_to(ope_b200_ctx* ctx, const void* h_in, float* 
 /* Waits until h_in of `ticket` has been copied to the device (the caller may
  * then reuse it); timeout_ms < 0 waits without limit. */
 OPE_B200_API int ope_b200_input_released(ope_b200_ctx* ctx, uint64_t ticket, int32_t timeout_ms);
+/* The device copy of a submitted frame's input (its ring slot), for more work
+ * on the same data on another stream (a per-chunk dispersion fit) without a
+ * second transfer: makes `stream` wait for the frame's input copy and returns
+ * the slot's device address. Valid until ope_b200_release(ticket); work that
+ * reads it must have finished by then (the slot takes a later frame). */
+OPE_B200_API int ope_b200_frame_device_input(ope_b200_ctx* ctx, uint64_t ticket, void* stream, const void** d_in);
 /* Waits for the frame; *h_out points at its A*B*(N/2) floats in pinned host
  * memory, valid until ope_b200_release(ticket). */
 OPE_B200_API int ope_b200_wait(ope_b200_ctx* ctx, uint64_t ticket, int32_t timeout_ms, const float** h_out);

@@ -58,6 +58,30 @@ def _ptr(t: Optional[torch.Tensor]):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+_CAI_TYPES = {torch.uint8: "|u1", torch.int16: "<i2", torch.float32: "<f4"}
+
+
+class _DeviceMemory:
+    """Device memory owned elsewhere, described by the CUDA array interface."""
+
+    def __init__(self, ptr: int, shape, dtype: torch.dtype):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": _CAI_TYPES[dtype],
+                                         "data": (int(ptr), False), "version": 2, "strides": None}
+
+
+def frame_input_view(ctx, ticket: int, ascans: int, stream=None) -> torch.Tensor:
+    """The first `ascans` raw A-scans of a submitted ring frame, as a device
+    tensor over the ring slot's own copy (no transfer). `stream` (default: the
+    current one) waits for the frame's input copy. The view is valid until
+    the frame is released; work reading it must have finished by then."""
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    ptr = ctx.frame_device_input(ticket, stream.cuda_stream)
+    dtype = {1: torch.uint8, 2: torch.int16, 9: torch.float32}[ctx.cfg.input_dtype]
+    return torch.as_tensor(_DeviceMemory(ptr, (ascans, ctx.cfg.signal_length), dtype),
+                           device=torch.device("cuda", ctx.cfg.device))
+
+
 def _stream(stream) -> ctypes.c_void_p:
     if stream is None:
         stream = torch.cuda.current_stream()

@@ -100,6 +100,7 @@ SIGNATURES = {
     "ope_b200_submit": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "ope_b200_submit_to": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "ope_b200_input_released": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32]),
+    "ope_b200_frame_device_input": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_void_p)]),
     "ope_b200_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(_FP)]),
     "ope_b200_release": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "ope_b200_request_fpn_determination": (ctypes.c_int, [_P]),
@@ -303,6 +304,13 @@ class Context:
 
     def input_released(self, ticket: int, timeout_ms: int = -1) -> None:
         self.check(lib().ope_b200_input_released(self.h, ticket, timeout_ms))
+
+    def frame_device_input(self, ticket: int, stream_handle: int) -> int:
+        """Device address of a submitted frame's input copy; the stream waits for it.
+        Valid until release(ticket)."""
+        p = ctypes.c_void_p(0)
+        self.check(lib().ope_b200_frame_device_input(self.h, ticket, stream_handle, ctypes.byref(p)))
+        return int(p.value)
 
     def wait(self, ticket: int, timeout_ms: int = -1) -> np.ndarray:
         """Waits for the frame; returns a zero-copy view of its output (valid until release)."""

@@ -905,6 +905,18 @@ int ope_b200_input_released(ope_b200_ctx* c, uint64_t ticket, int32_t timeout_ms
     return OPE_B200_OK;
 }
 
+int ope_b200_frame_device_input(ope_b200_ctx* c, uint64_t ticket, void* stream, const void** d_in) {
+    if (!c) return OPE_B200_E_INVALID;
+    if (!d_in) return fail(c, OPE_B200_E_INVALID, "null output pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    auto* r = find_slot(c, ticket);
+    if (!r) return fail(c, OPE_B200_E_INVALID, "unknown or released ticket");
+    OPE_CU(c, cudaSetDevice(c->device));
+    OPE_CU(c, cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), r->ev_in, 0));
+    *d_in = r->d_in;
+    return OPE_B200_OK;
+}
+
 int ope_b200_wait(ope_b200_ctx* c, uint64_t ticket, int32_t timeout_ms, const float** h_out) {
     if (!c) return OPE_B200_E_INVALID;
     cudaEvent_t ev;

@@ -96,6 +96,28 @@ def test_ring_submit_to_caller_buffers(cuda):
                 np.testing.assert_array_equal(outs[j].numpy(), want[j])
 
 
+def test_frame_device_input_is_the_submitted_frame(cuda):
+    import torch
+    from octproengine_b200.autofocus import frame_input_view
+    spec = _spec(n=1024, a=256, b=2)
+    frames = _frames(spec, 3, seed=41)
+    want = _reference_outputs(spec, frames)
+    side = torch.cuda.Stream()
+    with open_context(spec) as ctx:
+        pinned = [torch.from_numpy(f.view(np.uint8).reshape(-1).copy()).pin_memory() for f in frames]
+        tickets = [ctx.submit(p.data_ptr()) for p in pinned[:2]]
+        for k, t in enumerate(tickets):
+            view = frame_input_view(ctx, t, spec.num_ascans, side)  # side waits for the input copy
+            with torch.cuda.stream(side):
+                got = view.clone()
+            side.synchronize()
+            assert np.array_equal(got.cpu().numpy().view(np.uint16), frames[k].reshape(spec.num_ascans, -1))
+            np.testing.assert_array_equal(ctx.wait(t, 20000), want[k])
+            ctx.release(t)
+        with pytest.raises(capi.B200Error):
+            ctx.frame_device_input(tickets[0], side.cuda_stream)  # released
+
+
 # ------------------------------------------------------- Python Processor API
 
 
