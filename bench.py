@@ -54,6 +54,21 @@ def algorithmic_bytes_per_ascan(n=N, in_bytes=2):
     return n * in_bytes + (n // 2) * 4
 
 
+def algorithmic_flops_per_ascan(n=N):
+    """Floating-point operations one A-scan of the cubic chain needs: the
+    inverse DFT counted as 5 N log2 N (the conventional FFT count), the
+    reference's cubic Hermite formula 19 per sample (a: 4, b: 6, c: 1, pos^2: 1,
+    the Horner evaluation and + y1: 7), window 1 and phase 2 per sample, and per
+    output bin FPN 2, |X|^2 3, log 1 and the grayscale affine 4. 167 936 at
+    N = 2048."""
+    return 5 * n * int(np.log2(n)) + n * (19 + 3) + (n // 2) * (2 + 3 + 1 + 4)
+
+
+def fp32_peak_tflops(sm_mhz):
+    """Nominal FP32 peak: 148 SMs x 128 FP32 lanes x 2 (FMA) x SM clock."""
+    return 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -691,6 +706,9 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    clocks = clk.summary()
+    fp32_achieved = M * algorithmic_flops_per_ascan() / (kernel_ms / 1e3) / 1e12
+    fp32_peak = fp32_peak_tflops(clocks.get("sm_mhz"))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -701,11 +719,14 @@ def run_ours(args):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (tpa * M) if tpa else None,
                      "algorithmic_bytes": bytes_launch},
+        "roofline_fp32": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                          "frac": fp32_achieved / fp32_peak, "flops_per_ascan": algorithmic_flops_per_ascan(),
+                          "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x 2 (FMA) x median sampled SM clock"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 2,
                 "d2h_bytes_per_step": M * (N // 2) * 4},
         "e2e_stream": e2e_stream,
         "gpu_launches": args.steps,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "variants": variants,
     }
     if autofocus:
