@@ -180,6 +180,15 @@ def test_misaligned_input_rejected(cuda):
         with pytest.raises(capi.B200Error) as ei:
             ctx.process_device(buf.data_ptr() + 2, out.data_ptr())
         assert ei.value.code == capi.E_INVALID
+        for bad_out in (out.data_ptr() + 2, 0):  # output not float-aligned; null output
+            with pytest.raises(capi.B200Error) as ei:
+                ctx.process_device(buf.data_ptr(), bad_out)
+            assert ei.value.code == capi.E_INVALID
+        with pytest.raises(capi.B200Error) as ei:  # an empty buffer is an error, as in the reference
+            ctx.process_device(buf.data_ptr(), out.data_ptr(), num_ascans=0)
+        assert ei.value.code == capi.E_INVALID
+        with pytest.raises(capi.B200Error):
+            ctx.process_device(0, out.data_ptr())  # null input
     finally:
         ctx.close()
 
