@@ -236,11 +236,15 @@ def run_reference(args):
     }
     if not args.no_cpu_baseline:
         rate, dt, ascans = cpu_reference_run(args.steps, args.warmup, threads)
+        rate1, _, _ = cpu_reference_run(3, 1, 1)  # one Processor on one core, as the reference runs
         line.update({
             "value": rate, "ms_per_step": 1e3 * dt / args.steps,
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{ascans} A-scans: {threads} reference CpuBackend instances in parallel, "
-                                       f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW"},
+                                       f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW",
+                             "single_instance": {"value": rate1, "cores": 1,
+                                                 "sample": "3 B-scans through one CpuBackend (its one worker "
+                                                           "thread)"}},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         })
     if not args.no_cuda_reference:
@@ -697,9 +701,12 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, dt, ascans = cpu_reference_run(1, 1, threads)
+        rate1, _, _ = cpu_reference_run(3, 1, 1)
         cpu_base = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                     "sample": f"{ascans} A-scans ({threads} reference CpuBackend instances x 1 B-scan of the "
-                              f"workload); FFT = project shim (float32 radix-2), not FFTW"}
+                              f"workload); FFT = project shim (float32 radix-2), not FFTW",
+                    "single_instance": {"value": rate1, "cores": 1,
+                                        "sample": "3 B-scans through one CpuBackend (its one worker thread)"}}
     ctx.close()
     if dist is not None:
         dist.barrier()
