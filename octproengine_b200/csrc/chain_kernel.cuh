@@ -127,7 +127,8 @@ struct Layout {
     using sum_t = typename InTraits<DT>::sum_t;
     using raw_t = typename InTraits<DT>::raw_t;
     static constexpr int SPEC_BYTES = (N + 2 * SPEC_PAD) * 8;        // float2 pairs
-    static constexpr int PFX_BYTES = (N + 1) * 2 * (int)sizeof(sum_t);  // prefix sums, 2 rows
+    // prefix sums, 2 rows, one pad word per 32 (pfx_idx): conflict-free writes and reads
+    static constexpr int PFX_BYTES = ((N + 1) * 2 + ((N + 1) * 2) / 32 + 1) * (int)sizeof(sum_t);
     static constexpr int EXCH_BYTES_RAW = Plan<N>::EXCH_ELEMS * 16;
     static constexpr int WORK_BYTES = (EXCH_BYTES_RAW > SPEC_BYTES + PFX_BYTES + 256)
                                           ? EXCH_BYTES_RAW
@@ -424,50 +425,113 @@ OPE_HD void phase_store_packed(int t, const uint32_t* words, uint32_t* specw) {
 // x[i-(W-1) .. min(i+W, N-1)]. Window sums come from exact integer prefix sums
 // (the reference accumulates them in float; for integer input whose running
 // sum stays below 2^24 both are identical).
+//
+// Prefix-sum word w (2*i + row) lives at pfx_idx(w): one pad word per 32 puts
+// the 16-sample segments of consecutive threads, and the window ends that
+// consecutive threads read, in distinct banks.
+OPE_HD int pfx_idx(int w) { return w + (w >> 5); }
+
+// The 16 samples [16t, 16t+16) of both rows, widened to the sum type (device:
+// 16-byte shared loads).
+template <int N, int DT>
+OPE_HD void load_raw16(const unsigned char* stage, int t, typename InTraits<DT>::sum_t* xa,
+                       typename InTraits<DT>::sum_t* xb) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    using sum_t = typename InTraits<DT>::sum_t;
+    const raw_t* ra = reinterpret_cast<const raw_t*>(stage) + 16 * t;
+    const raw_t* rb = ra + N;
+#if defined(__CUDA_ARCH__)
+    constexpr int Q = (int)sizeof(raw_t);  // 16-byte words per 16 samples
+    uint4 qa[Q], qb[Q];
+#pragma unroll
+    for (int w = 0; w < Q; ++w) {
+        qa[w] = reinterpret_cast<const uint4*>(ra)[w];
+        qb[w] = reinterpret_cast<const uint4*>(rb)[w];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int e = k * Q;  // byte offset of sample k
+        const uint4& wa = qa[e >> 4];
+        const uint4& wb = qb[e >> 4];
+        const int lane = (e >> 2) & 3;
+        const unsigned ua = lane == 0 ? wa.x : lane == 1 ? wa.y : lane == 2 ? wa.z : wa.w;
+        const unsigned ub = lane == 0 ? wb.x : lane == 1 ? wb.y : lane == 2 ? wb.z : wb.w;
+        if constexpr (DT == IN_U8) {
+            xa[k] = (sum_t)((ua >> (8 * (k & 3))) & 0xFFu);
+            xb[k] = (sum_t)((ub >> (8 * (k & 3))) & 0xFFu);
+        } else if constexpr (DT == IN_U16) {
+            xa[k] = (sum_t)((ua >> (16 * (k & 1))) & 0xFFFFu);
+            xb[k] = (sum_t)((ub >> (16 * (k & 1))) & 0xFFFFu);
+        } else if constexpr (DT == IN_U32) {
+            xa[k] = (sum_t)ua;
+            xb[k] = (sum_t)ub;
+        } else {
+            xa[k] = (sum_t)__uint_as_float(ua);
+            xb[k] = (sum_t)__uint_as_float(ub);
+        }
+    }
+#else
+    for (int k = 0; k < 16; ++k) {
+        xa[k] = (sum_t)ra[k];
+        xb[k] = (sum_t)rb[k];
+    }
+#endif
+}
+
 // Step A: thread t owns samples [16t, 16t+16); returns its two row totals.
 template <int N, int DT>
 OPE_HD void phase_dc_local(int t, const unsigned char* stage, typename InTraits<DT>::sum_t* tot_a,
                            typename InTraits<DT>::sum_t* tot_b) {
     using sum_t = typename InTraits<DT>::sum_t;
+    sum_t xa[16], xb[16];
+    load_raw16<N, DT>(stage, t, xa, xb);
     sum_t sa = 0, sb = 0;
-    for (int i = 16 * t; i < 16 * t + 16; ++i) {
-        sum_t a, b;
-        load_raw_pair<DT>(stage, N, i, a, b);
-        sa += a;
-        sb += b;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        sa += xa[k];
+        sb += xb[k];
     }
     *tot_a = sa;
     *tot_b = sb;
 }
 
 // Step B: with the exclusive prefix of the totals, write prefix sums
-// pfx[2*i + row] = sum_{k < i} x_row[k] for i in [16t, 16t+16] (pfx[0] = 0).
+// P_row(i) = sum_{k < i} x_row[k] for i in [16t, 16t+16] (P(0) = 0) to word
+// pfx_idx(2*i + row).
 template <int N, int DT>
 OPE_HD void phase_dc_prefix(int t, const unsigned char* stage, typename InTraits<DT>::sum_t ex_a,
                             typename InTraits<DT>::sum_t ex_b, typename InTraits<DT>::sum_t* pfx) {
     using sum_t = typename InTraits<DT>::sum_t;
+    sum_t xa[16], xb[16];
+    load_raw16<N, DT>(stage, t, xa, xb);
     sum_t sa = ex_a, sb = ex_b;
     if (t == 0) {
-        pfx[0] = 0;
-        pfx[1] = 0;
+        pfx[pfx_idx(0)] = 0;
+        pfx[pfx_idx(1)] = 0;
     }
-    for (int i = 16 * t; i < 16 * t + 16; ++i) {
-        sum_t a, b;
-        load_raw_pair<DT>(stage, N, i, a, b);
-        sa += a;
-        sb += b;
-        OPE_SMEM_CHECK(2 * (i + 1) + 1 < 2 * (N + 1));
-        pfx[2 * (i + 1)] = sa;
-        pfx[2 * (i + 1) + 1] = sb;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int i = 16 * t + k;
+        sa += xa[k];
+        sb += xb[k];
+        OPE_SMEM_CHECK(pfx_idx(2 * (i + 1) + 1) < pfx_idx(2 * (N + 1)));
+        pfx[pfx_idx(2 * (i + 1))] = sa;
+        pfx[pfx_idx(2 * (i + 1) + 1)] = sb;
     }
 }
 
-// Step C: subtract the window means and write the spectrum pairs.
+// Step C: subtract the window means and write the spectrum pairs. A window of
+// a power-of-two count (the interior, when 2W is one: W = 64 by default) is
+// divided by multiplying with its exact reciprocal, which equals the correctly
+// rounded quotient; other counts use the correctly rounded division.
 template <int N, int DT>
 OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InTraits<DT>::sum_t* pfx,
                            int W, float2* spec) {
     using sum_t = typename InTraits<DT>::sum_t;
     constexpr int T = Plan<N>::T;
+    const int full = 2 * W;
+    const bool full_pow2 = (full & (full - 1)) == 0;
+    const float full_inv = 1.0f / (float)full;  // exact when full is a power of two
 #pragma unroll
     for (int c = t; c < N / 8; c += T) {
         float2 v[8];
@@ -477,16 +541,23 @@ OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InT
             int i = 8 * c + k;
             int start = (i >= W - 1) ? i - (W - 1) : 0;
             int end = (i + W < N - 1) ? i + W : N - 1;
-            sum_t sa = pfx[2 * (end + 1)] - pfx[2 * start];
-            sum_t sb = pfx[2 * (end + 1) + 1] - pfx[2 * start + 1];
-            float cnt = (float)(end - start + 1);
+            sum_t sa = pfx[pfx_idx(2 * (end + 1))] - pfx[pfx_idx(2 * start)];
+            sum_t sb = pfx[pfx_idx(2 * (end + 1) + 1)] - pfx[pfx_idx(2 * start + 1)];
+            const int n = end - start + 1;
+            float ma, mb;
+            if (full_pow2 && n == full) {
+                ma = (float)sa * full_inv;
+                mb = (float)sb * full_inv;
+            } else {
+                float cnt = (float)n;
 #if defined(__CUDA_ARCH__)
-            float ma = __fdiv_rn((float)sa, cnt);
-            float mb = __fdiv_rn((float)sb, cnt);
+                ma = __fdiv_rn((float)sa, cnt);
+                mb = __fdiv_rn((float)sb, cnt);
 #else
-            float ma = (float)sa / cnt;
-            float mb = (float)sb / cnt;
+                ma = (float)sa / cnt;
+                mb = (float)sb / cnt;
 #endif
+            }
             v[k] = sub2(v[k], make_float2(ma, mb));
         }
 #pragma unroll

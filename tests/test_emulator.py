@@ -90,10 +90,13 @@ def test_dc_removal_exact_rolling_mean(emu, n):
     assert err_gpu <= err_ref
 
 
-def test_dc_removal_small_sums_bit_exact(emu):
+@pytest.mark.parametrize("window", [32, 50, 7])
+def test_dc_removal_small_sums_bit_exact(emu, window):
     """While the reference's float prefix sum stays below 2^24 it is exact and
-    both agree bit for bit (uint8 input)."""
-    spec = spec_for(1024, LINEAR, dtype=UINT8, m=4, dc_removal=True, dc_window=32)
+    both agree bit for bit (uint8 input). Windows of 2W = 64 (a power of two:
+    the interior mean is a multiplication by the exact reciprocal), 100 and 14
+    (divisions)."""
+    spec = spec_for(1024, LINEAR, dtype=UINT8, m=4, dc_removal=True, dc_window=window)
     raw = H.random_raw(spec, seed=9)
     assert np.array_equal(H.emu_run(emu, spec, raw, "resampled"), oracle_resampled(spec, raw))
 
