@@ -127,8 +127,10 @@ struct Layout {
     using sum_t = typename InTraits<DT>::sum_t;
     using raw_t = typename InTraits<DT>::raw_t;
     static constexpr int SPEC_BYTES = (N + 2 * SPEC_PAD) * 8;        // float2 pairs
-    // prefix sums, 2 rows, one pad word per 32 (pfx_idx): conflict-free writes and reads
-    static constexpr int PFX_BYTES = ((N + 1) * 2 + ((N + 1) * 2) / 32 + 1) * (int)sizeof(sum_t);
+    // prefix sums, 2 rows, one pad word per 32 (pfx_idx): conflict-free writes and reads;
+    // rounded to 16 bytes so that the scan scratch after it holds doubles aligned
+    static constexpr int PFX_BYTES =
+        (((N + 1) * 2 + ((N + 1) * 2) / 32 + 1) * (int)sizeof(sum_t) + 15) / 16 * 16;
     static constexpr int EXCH_BYTES_RAW = Plan<N>::EXCH_ELEMS * 16;
     static constexpr int WORK_BYTES = (EXCH_BYTES_RAW > SPEC_BYTES + PFX_BYTES + 256)
                                           ? EXCH_BYTES_RAW
@@ -141,6 +143,8 @@ struct Layout {
     static constexpr int OFF_STAGE = ((WORK_BYTES + 127) / 128) * 128;
     static constexpr int OFF_MBAR = OFF_STAGE + STAGE_BYTES;  // one stage: refilled once unpacked
     static constexpr int TOTAL = OFF_MBAR + 64;
+    static_assert(OFF_PFX % 16 == 0 && OFF_SCAN % 16 == 0 && OFF_STAGE % 128 == 0 && OFF_MBAR % 16 == 0,
+                  "shared-memory regions must stay aligned for their widest accesses");
 };
 
 // ------------------------------------------------------------------ unpack --
