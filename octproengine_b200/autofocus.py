@@ -289,9 +289,73 @@ class FitEvaluator:
         return float(self.h_hs[0]), g
 
 
+def _allreduce_sum(values: np.ndarray, group=None) -> np.ndarray:
+    """Sum over the ranks of `group` in float64 (on the device under NCCL, on the host under gloo)."""
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.as_tensor(np.asarray(values, np.float64)).to(dev)
+    dist.all_reduce(t, group=group)
+    return t.cpu().numpy()
+
+
+def combine_entropy(h_local: float, s_local: float, group=None) -> tuple:
+    """Global (H, S) of the normalised intensity over every rank's bins from each
+    rank's own (H_r, S_r): S = sum S_r and sum I ln I = sum S_r (ln S_r - H_r),
+    H = ln S - (sum I ln I) / S."""
+    ilni = s_local * (np.log(s_local) - h_local) if s_local > 0 else 0.0
+    S, IlnI = _allreduce_sum(np.array([s_local, ilni]), group)
+    return float(np.log(S) - IlnI / S), float(S)
+
+
+class DistributedFitEvaluator:
+    """H and dH/d(d2, d3) of the entropy over the A-scans of every rank of a
+    process group (one volume split across GPUs, each rank holding its own
+    B-scans). Per evaluation: the forward on this rank's A-scans gives (H_r,
+    S_r); one all-reduce of 2 values gives the global (H, S); the adjoint on
+    this rank's A-scans with the global (H, S) gives this rank's share of the
+    gradient; one all-reduce of 8 values sums the shares. Every rank gets the
+    same (H, g), so BFGS takes the same steps everywhere and the ranks issue
+    the same collectives. ``local_forward(p8) -> (H_r, S_r)`` and
+    ``local_backward(p8, H, S) -> g8`` run the chain on this rank's data
+    (by default the GPU kernels of ``af`` on ``raw``)."""
+
+    def __init__(self, kmap: Sequence[float], af: Optional[Autofocus] = None, raw: Optional[torch.Tensor] = None,
+                 group=None, local_forward=None, local_backward=None):
+        self.kmap = np.asarray(kmap, np.float32)
+        self.group = group
+        self.count = 0
+        if local_forward is None:
+            dev = raw.device
+            d_params = torch.empty(8, dtype=torch.float32, device=dev)
+            d_hs = torch.empty(2, dtype=torch.float64, device=dev)
+            d_grad = torch.empty(8, dtype=torch.float32, device=dev)
+
+            def local_forward(p8):
+                d_params.copy_(torch.from_numpy(p8.astype(np.float32)))
+                af.forward(raw, d_params, hs=d_hs)
+                h = d_hs.cpu().numpy()
+                return float(h[0]), float(h[1])
+
+            def local_backward(p8, H, S):
+                d_hs.copy_(torch.tensor([H, S], dtype=torch.float64))
+                af.backward(raw, d_params, d_grad, hs=d_hs)
+                return d_grad.cpu().numpy().astype(np.float64)
+        self.local_forward, self.local_backward = local_forward, local_backward
+
+    def __call__(self, theta: np.ndarray):
+        p8 = np.zeros(8, np.float64)
+        p8[:4] = dispersion_poly(theta[0], theta[1]).astype(np.float32)
+        p8[4:] = self.kmap
+        h_r, s_r = self.local_forward(p8)
+        H, S = combine_entropy(h_r, s_r, self.group)
+        g8 = _allreduce_sum(self.local_backward(p8, H, S), self.group)
+        self.count += 1
+        return H, CENTRED_TO_POLY.T @ g8[:4]
+
+
 def fit_dispersion(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], init=(0.0, 0.0),
                    max_iter: int = 60, step_tol: float = 1e-3, first_step: float = 2.0,
-                   graph: bool = True, evaluator: Optional[FitEvaluator] = None) -> FitResult:
+                   graph: bool = True, evaluator=None) -> FitResult:
     """Minimises the image entropy over the centred dispersion (d2, d3).
 
     BFGS with an Armijo backtracking line search on the host (2 x 2 inverse
@@ -300,15 +364,19 @@ def fit_dispersion(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], init
     happens before the clock starts). ``kmap`` holds the resampling
     coefficients c0..c3. Stops when a step moves less than ``step_tol`` (rad).
     ``evaluator``: a FitEvaluator built earlier for this handle, this tensor
-    and this k-map, reused instead of building (and capturing) a new one.
+    and this k-map, reused instead of building (and capturing) a new one; or a
+    DistributedFitEvaluator, which fits one dispersion to the A-scans of every
+    rank of its process group.
     """
     if evaluator is None:
         ev = FitEvaluator(af, raw, kmap, graph=graph)
     else:
         ev = evaluator
-        if ev.af is not af or ev.raw.data_ptr() != raw.data_ptr() or ev.raw.shape != raw.shape \
-                or not np.array_equal(ev.kmap, np.asarray(kmap, np.float32)):
-            raise ValueError("evaluator was built for another handle, tensor or k-map")
+        if not np.array_equal(ev.kmap, np.asarray(kmap, np.float32)):
+            raise ValueError("evaluator was built for another k-map")
+        if isinstance(ev, FitEvaluator) and (ev.af is not af or ev.raw.data_ptr() != raw.data_ptr()
+                                             or ev.raw.shape != raw.shape):
+            raise ValueError("evaluator was built for another handle or tensor")
     count0 = ev.count
     t0 = time.perf_counter()
     x = np.asarray(init, np.float64)
@@ -351,6 +419,15 @@ class SweepResult:
     seconds: float
     grid: np.ndarray  # (n2, n3) entropies
     capture_seconds: float = 0.0
+
+
+def fit_dispersion_distributed(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], group=None,
+                               **kw) -> FitResult:
+    """fit_dispersion over the A-scans of every rank of `group` (torch.distributed
+    process group, NCCL between GPUs): `raw` holds this rank's A-scans; every rank
+    returns the same result."""
+    ev = DistributedFitEvaluator(kmap, af=af, raw=raw, group=group)
+    return fit_dispersion(af, raw, kmap, evaluator=ev, **kw)
 
 
 def grid_sweep(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], d2_range=(-40.0, 40.0),

@@ -254,3 +254,29 @@ def test_small_copies_move_fit_parameters_without_copy_engines(cuda):
     assert np.array_equal(back.numpy().view(np.uint8), want)
     assert L.ope_b200_af_small_copy(ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(h.data_ptr()), 5000,
                                     s) == capi.E_INVALID
+
+
+@pytest.mark.gpu
+def test_distributed_fit_on_one_nccl_rank_equals_the_local_fit(cuda):
+    """The data-parallel fit's two all-reduces (entropy partial sums, gradient)
+    over NCCL: on one rank it must land where the single-process fit does."""
+    import socket
+    from datetime import timedelta
+    import torch.distributed as dist
+    from octproengine_b200.autofocus import fit_dispersion, fit_dispersion_distributed
+    raw_t, raw, window, ctrue = make_case(m=128, seed=41, d2=-18.0, d3=9.0)
+    af = _af(cuda, O.LANCZOS, window)
+    d_raw = raw_t.to(cuda)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=60), device_id=cuda)
+    try:
+        got = fit_dispersion_distributed(af, d_raw, ctrue)
+    finally:
+        dist.destroy_process_group()
+    want = fit_dispersion(af, d_raw, ctrue)
+    assert abs(got.d2 - want.d2) < 1e-4 and abs(got.d3 - want.d3) < 1e-4, (got, want)
+    assert got.entropy == pytest.approx(want.entropy, rel=1e-9)

@@ -72,3 +72,99 @@ def test_rank_setup_reads_torchrun_environment():
         bscan_range(10, 2, 2)
     with pytest.raises(ValueError):
         weak_scaling_rate(1.0, 0.0, 1)
+
+
+# ---------------------------------------------- data-parallel dispersion fit
+
+
+def _af_case():
+    import numpy as np
+    from octproengine_b200 import synth
+    from oracle import restate as R
+    n = 2048
+    ctrue = synth.linearising_coeffs(n)
+    raw = synth.as_numpy(synth.generate(synth.SynthParams(n=n, ascans=48, seed=31, d2=14.0, d3=-6.0,
+                                                          resampling_truth=ctrue)), "uint16")
+    return raw, R.window_curve(n, R.HANN, 0.5, 0.95), np.asarray(ctrue)
+
+
+def _oracle_fns(raw, win):
+    """This rank's forward and adjoint, in float64 (the oracle chain, Lanczos-8)."""
+    import numpy as np
+    import torch
+    from oracle import autofocus64 as O
+
+    def fwd(p8):
+        I, _ = O.intensity(raw, p8, win, O.LANCZOS)
+        return float(O.entropy_of(I)), float(I.sum())
+
+    def bwd(p8, H, S):
+        I, p = O.intensity(raw, p8, win, O.LANCZOS, requires_grad=True)
+        G = torch.where(I > 0, -(torch.log(I.detach() / S) + H) / S, torch.zeros_like(I))
+        (g,) = torch.autograd.grad((G * I).sum(), p)
+        return g.numpy()
+    return fwd, bwd
+
+
+class _WholeVolume:
+    """The same objective on all A-scans in one process (no collective)."""
+
+    def __init__(self, raw, win, kmap):
+        import numpy as np
+        self.raw, self.win, self.kmap, self.count = raw, win, np.asarray(kmap, np.float32), 0
+
+    def __call__(self, theta):
+        import numpy as np
+        from octproengine_b200.autofocus import CENTRED_TO_POLY, dispersion_poly
+        from oracle import autofocus64 as O
+        p8 = np.zeros(8)
+        p8[:4] = dispersion_poly(theta[0], theta[1]).astype(np.float32)
+        p8[4:] = self.kmap
+        H, g = O.entropy_and_grad(self.raw, p8, self.win, O.LANCZOS)
+        self.count += 1
+        return H, CENTRED_TO_POLY.T @ g[:4]
+
+
+def _fit_worker(rank, world, port, q):
+    import numpy as np
+    import torch.distributed as dist
+    from datetime import timedelta
+    from octproengine_b200.autofocus import DistributedFitEvaluator, fit_dispersion
+    from octproengine_b200.multirank import bscan_range
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=120))
+    try:
+        raw, win, kmap = _af_case()
+        first, count = bscan_range(raw.shape[0], world, rank)  # A-scans split like B-scans
+        fwd, bwd = _oracle_fns(raw[first:first + count], win)
+        ev = DistributedFitEvaluator(kmap, local_forward=fwd, local_backward=bwd)
+        H, g = ev(np.array([9.0, -2.0]))
+        fit = fit_dispersion(None, None, kmap, evaluator=ev, max_iter=4)
+        q.put((rank, H, tuple(g), fit.d2, fit.d3, fit.evaluations))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_distributed_fit_equals_the_whole_volume_fit():
+    import multiprocessing as mp
+    import numpy as np
+    from octproengine_b200.autofocus import fit_dispersion
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fit_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    res = sorted(q.get(timeout=5) for _ in range(2))
+    raw, win, kmap = _af_case()
+    whole = _WholeVolume(raw, win, kmap)
+    H, g = whole(np.array([9.0, -2.0]))
+    fit = fit_dispersion(None, None, kmap, evaluator=whole, max_iter=4)
+    for r in res:
+        assert r[1] == pytest.approx(H, rel=1e-12)
+        assert np.allclose(r[2], g, rtol=1e-8, atol=1e-12 * np.abs(g).max())
+        assert (r[3], r[4], r[5]) == pytest.approx((fit.d2, fit.d3, fit.evaluations), rel=1e-6)
+    assert res[0][3:] == res[1][3:]  # both ranks took the same steps
