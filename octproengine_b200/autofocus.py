@@ -298,13 +298,22 @@ def _allreduce_sum(values: np.ndarray, group=None) -> np.ndarray:
     return t.cpu().numpy()
 
 
+def entropy_parts(h_local: float, s_local: float) -> np.ndarray:
+    """(S_r, sum I ln I over this rank's bins) from its own entropy: S_r (ln S_r - H_r).
+    A rank without data contributes (0, 0)."""
+    return np.array([s_local, s_local * (np.log(s_local) - h_local) if s_local > 0 else 0.0])
+
+
+def entropy_from_parts(parts: np.ndarray) -> tuple:
+    """(H, S) from the summed parts: H = ln S - (sum I ln I) / S."""
+    S, IlnI = float(parts[0]), float(parts[1])
+    return float(np.log(S) - IlnI / S), S
+
+
 def combine_entropy(h_local: float, s_local: float, group=None) -> tuple:
     """Global (H, S) of the normalised intensity over every rank's bins from each
-    rank's own (H_r, S_r): S = sum S_r and sum I ln I = sum S_r (ln S_r - H_r),
-    H = ln S - (sum I ln I) / S."""
-    ilni = s_local * (np.log(s_local) - h_local) if s_local > 0 else 0.0
-    S, IlnI = _allreduce_sum(np.array([s_local, ilni]), group)
-    return float(np.log(S) - IlnI / S), float(S)
+    rank's own (H_r, S_r): one all-reduce of the two parts."""
+    return entropy_from_parts(_allreduce_sum(entropy_parts(h_local, s_local), group))
 
 
 class DistributedFitEvaluator:
@@ -330,13 +339,19 @@ class DistributedFitEvaluator:
             d_hs = torch.empty(2, dtype=torch.float64, device=dev)
             d_grad = torch.empty(8, dtype=torch.float32, device=dev)
 
+            empty = raw.shape[0] == 0  # a rank without A-scans still joins every collective
+
             def local_forward(p8):
+                if empty:
+                    return 0.0, 0.0
                 d_params.copy_(torch.from_numpy(p8.astype(np.float32)))
                 af.forward(raw, d_params, hs=d_hs)
                 h = d_hs.cpu().numpy()
                 return float(h[0]), float(h[1])
 
             def local_backward(p8, H, S):
+                if empty:
+                    return np.zeros(8)
                 d_hs.copy_(torch.tensor([H, S], dtype=torch.float64))
                 af.backward(raw, d_params, d_grad, hs=d_hs)
                 return d_grad.cpu().numpy().astype(np.float64)

@@ -168,3 +168,19 @@ def test_distributed_fit_equals_the_whole_volume_fit():
         assert np.allclose(r[2], g, rtol=1e-8, atol=1e-12 * np.abs(g).max())
         assert (r[3], r[4], r[5]) == pytest.approx((fit.d2, fit.d3, fit.evaluations), rel=1e-6)
     assert res[0][3:] == res[1][3:]  # both ranks took the same steps
+
+
+def test_entropy_parts_of_a_split_volume_sum_to_the_whole():
+    import numpy as np
+    from octproengine_b200.autofocus import entropy_from_parts, entropy_parts
+    rng = np.random.default_rng(3)
+    I = rng.gamma(0.3, 5.0, size=(40, 512))
+
+    def h_s(x):
+        S = x.sum()
+        p = x / S
+        return float(-(p * np.log(p)).sum()), float(S)
+    whole = h_s(I)
+    parts = sum(entropy_parts(*h_s(I[a:b])) for a, b in ((0, 13), (13, 40))) + entropy_parts(0.0, 0.0)
+    H, S = entropy_from_parts(parts)
+    assert H == pytest.approx(whole[0], rel=1e-13) and S == pytest.approx(whole[1], rel=1e-14)
