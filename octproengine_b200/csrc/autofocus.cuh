@@ -115,7 +115,7 @@ struct AfForwardSink {
 };
 
 template <int N, int DT, int INTERP>
-__global__ void __launch_bounds__(N / 16, 3) af_forward_kernel(const AfArgs a) {
+__global__ void __launch_bounds__(N / 16, 8192 / N) af_forward_kernel(const AfArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     using LY = Layout<N, DT>;
     AfForwardSink<N> sink;
