@@ -244,6 +244,14 @@ OPE_B200_API int ope_b200_af_forward(ope_b200_af* af, const void* d_in, int64_t 
 OPE_B200_API int ope_b200_af_backward(ope_b200_af* af, const void* d_in, int64_t num_ascans, const float* d_params,
                                       int32_t output_mode, const float* d_grad_out, const double* d_hs,
                                       float* d_grad_params, void* stream);
+/* Same as ope_b200_af_backward for the dispersion coefficients d0..d3 only
+ * (entries 4..7, the k-map, are written as 0): the adjoint keeps the resampled
+ * samples instead of differentiating the interpolation, which a dispersion
+ * fit does not need. */
+OPE_B200_API int ope_b200_af_backward_dispersion(ope_b200_af* af, const void* d_in, int64_t num_ascans,
+                                                 const float* d_params, int32_t output_mode,
+                                                 const float* d_grad_out, const double* d_hs,
+                                                 float* d_grad_params, void* stream);
 /* 1 when kernels can use `ptr` at that address (device memory, or page-locked
  * host memory under unified addressing), else 0. */
 OPE_B200_API int ope_b200_af_kernel_accessible(const void* ptr);

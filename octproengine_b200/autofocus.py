@@ -151,15 +151,17 @@ class Autofocus:
 
     def backward(self, raw: torch.Tensor, params: torch.Tensor, grad: torch.Tensor,
                  grad_out: Optional[torch.Tensor] = None, hs: Optional[torch.Tensor] = None,
-                 output: int = OUT_INTENSITY, stream=None) -> None:
-        """dL/dparams into ``grad`` (8 float32): L = sum(grad_out * image) or L = H."""
+                 output: int = OUT_INTENSITY, stream=None, dispersion_only: bool = False) -> None:
+        """dL/dparams into ``grad`` (8 float32): L = sum(grad_out * image) or L = H.
+        ``dispersion_only``: d0..d3 only (the k-map entries are 0), a cheaper adjoint."""
         m = self._check_raw(raw)
         self._check_params(params)
         if grad_out is not None and (grad_out.dtype != torch.float32 or not grad_out.is_contiguous()
                                      or grad_out.shape != (m, self.n // 2)):
             raise ValueError("grad_out must be a contiguous float32 (A-scans, N/2) tensor")
-        self._check(capi.lib().ope_b200_af_backward(self.h, _ptr(raw), m, _ptr(params), output, _ptr(grad_out),
-                                                    _ptr(hs), _ptr(grad), _stream(stream)))
+        f = capi.lib().ope_b200_af_backward_dispersion if dispersion_only else capi.lib().ope_b200_af_backward
+        self._check(f(self.h, _ptr(raw), m, _ptr(params), output, _ptr(grad_out), _ptr(hs), _ptr(grad),
+                      _stream(stream)))
 
 
 class ChainImage(torch.autograd.Function):
@@ -273,7 +275,7 @@ class FitEvaluator:
     def _enqueue(self, stream) -> None:
         self._copy(self.d_params, self.h_params, stream)
         self.af.forward(self.raw, self.d_params, hs=self.d_hs, stream=stream)
-        self.af.backward(self.raw, self.d_params, self.d_grad, hs=self.d_hs, stream=stream)
+        self.af.backward(self.raw, self.d_params, self.d_grad, hs=self.d_hs, stream=stream, dispersion_only=True)
         self._copy(self.h_hs, self.d_hs, stream)
         self._copy(self.h_grad, self.d_grad, stream)
 
@@ -353,7 +355,7 @@ class DistributedFitEvaluator:
                 if empty:
                     return np.zeros(8)
                 d_hs.copy_(torch.tensor([H, S], dtype=torch.float64))
-                af.backward(raw, d_params, d_grad, hs=d_hs)
+                af.backward(raw, d_params, d_grad, hs=d_hs, dispersion_only=True)
                 return d_grad.cpu().numpy().astype(np.float64)
         self.local_forward, self.local_backward = local_forward, local_backward
 

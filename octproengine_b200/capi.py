@@ -122,6 +122,8 @@ SIGNATURES = {
     "ope_b200_af_last_error": (ctypes.c_char_p, [_P]),
     "ope_b200_af_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P]),
     "ope_b200_af_backward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P, _P]),
+    "ope_b200_af_backward_dispersion": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P,
+                                                        _P]),
     "ope_b200_af_kernel_accessible": (ctypes.c_int, [_P]),
     "ope_b200_af_small_copy": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P]),
     "ope_b200_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(_P)]),

@@ -335,9 +335,9 @@ int ope_b200_af_forward(ope_b200_af* o, const void* d_in, int64_t num_ascans, co
     return OPE_B200_OK;
 }
 
-int ope_b200_af_backward(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float* d_params,
-                         int32_t output_mode, const float* d_grad_out, const double* d_hs, float* d_grad_params,
-                         void* stream) {
+static int af_backward_impl(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float* d_params,
+                            int32_t output_mode, const float* d_grad_out, const double* d_hs, float* d_grad_params,
+                            void* stream, bool disp_only) {
     if (!o) return OPE_B200_E_INVALID;
     if (!d_grad_params) return af_fail(o, OPE_B200_E_INVALID, "null gradient output");
     if (!d_grad_out && !d_hs)
@@ -346,16 +346,31 @@ int ope_b200_af_backward(ope_b200_af* o, const void* d_in, int64_t num_ascans, c
         return af_fail(o, OPE_B200_E_INVALID, "output_mode must be 1 (intensity) or 2 (dB)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     AfArgs a;
-    int rc = af_prepare(o, d_in, num_ascans, d_params, s, true, &a);
+    int rc = af_prepare(o, d_in, num_ascans, d_params, s, !disp_only, &a);  // no dy tables when dispersion-only
     if (rc != OPE_B200_OK) return rc;
     a.grad_out = d_grad_out;
     a.out_mode = d_grad_out ? output_mode : AF_OUT_NONE;
     a.hs = d_hs;
+    a.disp_only = disp_only ? 1 : 0;
     int grid = 0;
     AF_CU(o, af_launch(true, o, a, s, &grid));
     af_grad_finalize<<<1, 256, 0, s>>>(o->partial, grid, d_grad_params);
     AF_CU(o, cudaGetLastError());
     return OPE_B200_OK;
+}
+
+int ope_b200_af_backward(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float* d_params,
+                         int32_t output_mode, const float* d_grad_out, const double* d_hs, float* d_grad_params,
+                         void* stream) {
+    return af_backward_impl(o, d_in, num_ascans, d_params, output_mode, d_grad_out, d_hs, d_grad_params, stream,
+                            false);
+}
+
+int ope_b200_af_backward_dispersion(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float* d_params,
+                                    int32_t output_mode, const float* d_grad_out, const double* d_hs,
+                                    float* d_grad_params, void* stream) {
+    return af_backward_impl(o, d_in, num_ascans, d_params, output_mode, d_grad_out, d_hs, d_grad_params, stream,
+                            true);
 }
 
 int ope_b200_af_kernel_accessible(const void* ptr) {

@@ -43,6 +43,7 @@ struct AfArgs {
     const float* grad_out;   // backward: dL/d(out), M x N/2; nullptr = entropy objective
     const double* hs;        // entropy objective: hs[0] = H, hs[1] = S
     double* partial;         // per-CTA partial sums (forward: 2, backward: 8 per CTA)
+    int disp_only;           // backward: dispersion gradients only (k-map entries left 0)
 };
 
 // ------------------------------------------------------------ tables ----
@@ -141,8 +142,40 @@ struct AfLayout {
     static constexpr int OFF_SPEC = ((2 * ROW_BYTES + 127) / 128) * 128;
     static constexpr int OFF_EXCH = ((OFF_SPEC + (N + 2 * SPEC_PAD) * 8 + 127) / 128) * 128;
     static constexpr int OFF_SCAN = OFF_EXCH + Plan<N>::EXCH_ELEMS * 16;
-    static constexpr int TOTAL = OFF_SCAN + 1024;
+    // the resampled samples y of the pair, kept for the dispersion-only adjoint
+    static constexpr int OFF_Y = OFF_SCAN + 1024;
+    static constexpr int TOTAL = OFF_Y + N * 8;
+    static_assert(OFF_SPEC % 128 == 0 && OFF_EXCH % 128 == 0 && OFF_SCAN % 16 == 0 && OFF_Y % 16 == 0,
+                  "shared-memory regions must stay aligned for their widest accesses");
 };
+
+// Interpolated value alone (the dispersion-only adjoint), same arithmetic as
+// af_interp_deriv's value.
+template <int N, int INTERP>
+__device__ __forceinline__ float2 af_interp_value(const float2* spec, const AfArgs& a, int j) {
+    if (INTERP == INTERP_LINEAR) {
+        const int2 e = a.c.lin[j];
+        const float2 y1 = spec[e.x], y2 = spec[e.x + 1];
+        return fma2(sub2(y2, y1), dup2(__int_as_float(e.y)), y1);
+    } else if (INTERP == INTERP_CUBIC) {
+        const int2 e = a.c.cub[j];
+        const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
+        const float pos = __int_as_float(e.y);
+        const float2 y0 = spec[i0], y1 = spec[i1], y2 = spec[i1 + 1], y3 = spec[i1 + 2];
+        const float2 ca = add2(sub2(mul2(dup2(3.0f), sub2(y1, y2)), y0), y3);
+        const float2 cb = sub2(add2(sub2(mul2(dup2(2.0f), y0), mul2(dup2(5.0f), y1)), mul2(dup2(4.0f), y2)), y3);
+        const float2 cc = sub2(y2, y0);
+        const float2 P = dup2(pos);
+        return fma2(mul2(dup2(0.5f * pos), fma2(fma2(ca, P, cb), P, cc)), dup2(1.0f), y1);
+    } else if (INTERP == INTERP_LANCZOS) {
+        const int b = a.c.lz_base[j];
+        float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc = fma2(spec[b + k], dup2(__ldg(a.c.lz_w + k * N + j)), acc);
+        return acc;
+    }
+    return spec[SPEC_PAD + j];
+}
 
 // Interpolated value and its derivative with respect to the position, for
 // both A-scans of a pair, at output sample j.
@@ -222,6 +255,7 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
     float2* spec = reinterpret_cast<float2*>(smem + LY::OFF_SPEC);
     float4* exch = reinterpret_cast<float4*>(smem + LY::OFF_EXCH);
     double* scan = reinterpret_cast<double*>(smem + LY::OFF_SCAN);
+    float2* ybuf = reinterpret_cast<float2*>(smem + LY::OFF_Y);
     const int t = threadIdx.x;
     const ChainArgs& c = a.c;
     const long long m = c.m;
@@ -269,7 +303,19 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
         __syncthreads();
         // ---- recompute the forward up to X ----
         cp v[16];
-        phase_prestage<N, INTERP>(t, spec, c, v);
+        if (a.disp_only) {
+            // y kept in shared memory: the dispersion adjoint needs y, not dy/dr
+#pragma unroll
+            for (int s2 = 0; s2 < 16; ++s2) {
+                const int j = t + s2 * T;
+                const float2 y = af_interp_value<N, INTERP>(spec, a, j);
+                ybuf[j] = y;
+                const float2 q = __ldg(c.wph + j);
+                v[s2] = cpmake(mul2(y, dup2(q.x)), mul2(y, dup2(q.y)));
+            }
+        } else {
+            phase_prestage<N, INTERP>(t, spec, c, v);
+        }
         fft_twiddle_dft<N, 0>(t, v, c.tw);
         fft_store<N, 0>(t, v, exch);
         __syncthreads();
@@ -351,11 +397,16 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
                 const float2 hre = fma2(A.re, wc, neg2(mul2(A.im, ws)));
                 const float2 him = fma2(A.re, ws, mul2(A.im, wc));
                 float2 y, dy;
-                af_interp_deriv<N, INTERP>(spec, a, j, y, dy);
+                float gr = 0.0f;
+                if (a.disp_only) {
+                    y = ybuf[j];
+                } else {
+                    af_interp_deriv<N, INTERP>(spec, a, j, y, dy);
+                    const float2 gy2 = mul2(hre, dy);
+                    gr = (gy2.x + gy2.y) * __ldg(a.rmask + j);
+                }
                 const float2 gphi2 = neg2(mul2(y, him));
-                const float2 gy2 = mul2(hre, dy);
                 const float gphi = gphi2.x + gphi2.y;
-                const float gr = (gy2.x + gy2.y) * __ldg(a.rmask + j);
                 const float tj = (float)j * inv_nm1;
                 float p = 1.0f;
 #pragma unroll

@@ -280,3 +280,23 @@ def test_distributed_fit_on_one_nccl_rank_equals_the_local_fit(cuda):
     want = fit_dispersion(af, d_raw, ctrue)
     assert abs(got.d2 - want.d2) < 1e-4 and abs(got.d3 - want.d3) < 1e-4, (got, want)
     assert got.entropy == pytest.approx(want.entropy, rel=1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("interp", [O.LINEAR, O.CUBIC, O.LANCZOS])
+def test_dispersion_only_adjoint_matches_the_full_one(cuda, interp):
+    raw_t, raw, window, ctrue = make_case(m=96, seed=23)
+    p = params_of(11.0, -4.0, ctrue)
+    af = _af(cuda, interp, window)
+    d_raw = raw_t.to(cuda)
+    d_p = torch.from_numpy(p).to(cuda)
+    hs = torch.empty(2, dtype=torch.float64, device=cuda)
+    af.forward(d_raw, d_p, hs=hs)
+    full = torch.empty(8, dtype=torch.float32, device=cuda)
+    disp = torch.full((8,), float("nan"), dtype=torch.float32, device=cuda)
+    af.backward(d_raw, d_p, full, hs=hs)
+    af.backward(d_raw, d_p, disp, hs=hs, dispersion_only=True)
+    f, d = full.cpu().numpy().astype(np.float64), disp.cpu().numpy().astype(np.float64)
+    assert np.all(d[4:] == 0.0)
+    # the same adjoint up to the rounding of the recomputed resampled samples
+    assert np.allclose(d[:4], f[:4], rtol=1e-4, atol=1e-5 * np.abs(f[:4]).max()), (d, f)
