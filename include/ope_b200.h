@@ -247,7 +247,9 @@ OPE_B200_API int ope_b200_af_backward(ope_b200_af* af, const void* d_in, int64_t
 /* Same as ope_b200_af_backward for the dispersion coefficients d0..d3 only
  * (entries 4..7, the k-map, are written as 0): the adjoint keeps the resampled
  * samples instead of differentiating the interpolation, which a dispersion
- * fit does not need. */
+ * fit does not need. Called after ope_b200_af_forward on the same stream with
+ * the same d_params pointer, it reuses the device tables that forward built
+ * (the values behind d_params must not change between the two calls). */
 OPE_B200_API int ope_b200_af_backward_dispersion(ope_b200_af* af, const void* d_in, int64_t num_ascans,
                                                  const float* d_params, int32_t output_mode,
                                                  const float* d_grad_out, const double* d_hs,

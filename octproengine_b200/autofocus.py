@@ -275,9 +275,12 @@ class FitEvaluator:
     def _enqueue(self, stream) -> None:
         self._copy(self.d_params, self.h_params, stream)
         self.af.forward(self.raw, self.d_params, hs=self.d_hs, stream=stream)
-        self.af.backward(self.raw, self.d_params, self.d_grad, hs=self.d_hs, stream=stream, dispersion_only=True)
+        # the gradient's finalize kernel writes straight into page-locked host memory
+        grad = self.h_grad if self.sm_copies else self.d_grad
+        self.af.backward(self.raw, self.d_params, grad, hs=self.d_hs, stream=stream, dispersion_only=True)
         self._copy(self.h_hs, self.d_hs, stream)
-        self._copy(self.h_grad, self.d_grad, stream)
+        if not self.sm_copies:
+            self._copy(self.h_grad, self.d_grad, stream)
 
     def __call__(self, theta: np.ndarray):
         self._set(theta)

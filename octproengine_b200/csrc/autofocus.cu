@@ -156,6 +156,7 @@ struct ope_b200_af {
     float2* wph = nullptr;
     double* partial = nullptr;
     int cap = 0;
+    const float* tables_params = nullptr;  // parameter pointer the device tables were last built from
     std::string err;
 };
 
@@ -199,22 +200,27 @@ cudaError_t af_launch(bool backward, ope_b200_af* o, const AfArgs& args, cudaStr
     }
 }
 
+// build_tables: false reuses the tables of the previous call (same parameters,
+// stream-ordered after it).
 int af_prepare(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float* d_params, cudaStream_t s,
-               bool backward, AfArgs* args) {
+               bool backward, AfArgs* args, bool build_tables = true) {
     if (!d_in || !d_params) return af_fail(o, OPE_B200_E_INVALID, "null input or parameter pointer");
     if (num_ascans < 1) return af_fail(o, OPE_B200_E_INVALID, "num_ascans must be >= 1");
     if ((reinterpret_cast<uintptr_t>(d_in) & 15u) != 0)
         return af_fail(o, OPE_B200_E_INVALID, "input must be 16-byte aligned");
     AF_CU(o, cudaSetDevice(o->device));
-    const int threads = 256;
-    af_tables_kernel<<<(o->n + threads - 1) / threads, threads, 0, s>>>(o->n, o->interp, d_params, o->window, o->lin,
-                                                                         o->cub, o->lzb, o->lzw, o->lzdw, o->rmask,
-                                                                         o->wph);
-    AF_CU(o, cudaGetLastError());
-    if (o->interp == INTERP_LANCZOS) {
-        af_lanczos_kernel<<<(16 * o->n + threads - 1) / threads, threads, 0, s>>>(o->n, d_params, o->lzw,
-                                                                                 backward ? o->lzdw : nullptr);
+    if (build_tables) {
+        const int threads = 256;
+        af_tables_kernel<<<(o->n + threads - 1) / threads, threads, 0, s>>>(o->n, o->interp, d_params, o->window,
+                                                                             o->lin, o->cub, o->lzb, o->lzw, o->lzdw,
+                                                                             o->rmask, o->wph);
         AF_CU(o, cudaGetLastError());
+        if (o->interp == INTERP_LANCZOS) {
+            af_lanczos_kernel<<<(16 * o->n + threads - 1) / threads, threads, 0, s>>>(o->n, d_params, o->lzw,
+                                                                                     backward ? o->lzdw : nullptr);
+            AF_CU(o, cudaGetLastError());
+        }
+        o->tables_params = d_params;
     }
     AfArgs a{};
     a.c.in = d_in;
@@ -346,7 +352,10 @@ static int af_backward_impl(ope_b200_af* o, const void* d_in, int64_t num_ascans
         return af_fail(o, OPE_B200_E_INVALID, "output_mode must be 1 (intensity) or 2 (dB)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     AfArgs a;
-    int rc = af_prepare(o, d_in, num_ascans, d_params, s, !disp_only, &a);  // no dy tables when dispersion-only
+    // the dispersion-only adjoint needs no derivative tables: it reuses the
+    // forward's when they were built from the same parameter pointer
+    const bool reuse = disp_only && o->tables_params == d_params;
+    int rc = af_prepare(o, d_in, num_ascans, d_params, s, !disp_only, &a, !reuse);
     if (rc != OPE_B200_OK) return rc;
     a.grad_out = d_grad_out;
     a.out_mode = d_grad_out ? output_mode : AF_OUT_NONE;

@@ -300,3 +300,25 @@ def test_dispersion_only_adjoint_matches_the_full_one(cuda, interp):
     assert np.all(d[4:] == 0.0)
     # the same adjoint up to the rounding of the recomputed resampled samples
     assert np.allclose(d[:4], f[:4], rtol=1e-4, atol=1e-5 * np.abs(f[:4]).max()), (d, f)
+
+
+@pytest.mark.gpu
+def test_dispersion_only_adjoint_reuses_only_matching_tables(cuda):
+    """After a forward with the same parameter pointer the adjoint reuses its
+    tables; after a forward with another pointer it builds its own: the same
+    gradient either way."""
+    raw_t, raw, window, ctrue = make_case(m=64, seed=29)
+    af = _af(cuda, O.LANCZOS, window)
+    d_raw = raw_t.to(cuda)
+    A = torch.from_numpy(params_of(11.0, -4.0, ctrue)).to(cuda)
+    B = torch.from_numpy(params_of(-20.0, 7.0, ctrue)).to(cuda)
+    hs = torch.empty(2, dtype=torch.float64, device=cuda)
+    hsB = torch.empty(2, dtype=torch.float64, device=cuda)
+    g = [torch.empty(8, dtype=torch.float32, device=cuda) for _ in range(3)]
+    af.forward(d_raw, A, hs=hs)
+    af.backward(d_raw, A, g[0], hs=hs, dispersion_only=True)  # reuses the tables of A
+    af.forward(d_raw, B, hs=hsB)
+    af.backward(d_raw, A, g[1], hs=hs, dispersion_only=True)  # tables of B present: rebuilds for A
+    af.forward(d_raw, A, hs=hs)
+    af.backward(d_raw, A, g[2], hs=hs, dispersion_only=True)
+    assert torch.equal(g[0], g[1]) and torch.equal(g[0], g[2])
