@@ -61,7 +61,8 @@ typedef struct ope_b200_config {
     int32_t ascans_per_bscan;  /* DataParameters::ascansPerBscan (A)          */
     int32_t bscans_per_buffer; /* DataParameters::bscansPerBuffer (B)         */
     int32_t input_dtype;       /* DataParameters::inputDataType (ope::DataType) */
-    int32_t bitshift;          /* DataParameters::bitshift (CUDA backend only) */
+    int32_t bitshift;          /* DataParameters::bitshift: 8/16-bit samples >> 4 (the reference
+                                  CUDA backend's rule); ignored for 32-bit samples */
     int32_t resampling_enabled;
     int32_t interpolation; /* ope::InterpolationMethod */
     int32_t windowing_enabled;

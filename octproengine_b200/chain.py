@@ -53,6 +53,7 @@ class ChainSpec:
     fpn_continuous: bool = False
     bscan_flip: bool = False
     float32_as_uint32: bool = False
+    bitshift: bool = False  # 8/16-bit samples >> 4 before the chain
     dc_split: bool = True
     device: int = 0
     num_input_buffers: int = 2  # depth of the host frame ring
@@ -94,6 +95,7 @@ class ChainSpec:
         c.fpn_continuous = int(self.fpn_continuous)
         c.bscan_flip = int(self.bscan_flip)
         c.float32_as_uint32 = int(self.float32_as_uint32)
+        c.bitshift = int(self.bitshift)
         c.dc_split = int(self.dc_split)
         c.device = int(self.device)
         c.num_input_buffers = int(self.num_input_buffers)

@@ -295,6 +295,8 @@ static ChainArgs make_args(ope_b200_ctx* c, const void* d_in, float* d_out, long
     a.timeout_ns = 2000000000ull;
     a.neg_zero = -0.0f;
     a.dc_resp = s.has_dcr ? s.dcr : nullptr;
+    // 8/16-bit samples only; 32-bit samples ignore the flag, as the reference CPU backend does
+    a.bitshift = (c->cfg.bitshift && (c->in_kind == IN_U8 || c->in_kind == IN_U16)) ? 1 : 0;
     return a;
 }
 

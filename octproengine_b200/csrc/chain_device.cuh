@@ -285,6 +285,12 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
             return;
         }
         const unsigned char* stage = stages;
+        if constexpr (DT == IN_U8 || DT == IN_U16) {
+            if (a.bitshift) {
+                phase_bitshift<N, DT>(t, stages);
+                tm.sync();
+            }
+        }
 
         // ---- unpack (+ DC removal or exact DC split) ----
         float2 dc = make_float2(0.0f, 0.0f);

@@ -83,6 +83,7 @@ struct ChainArgs {
     // cpu_kernels.tpp:381-400): when set, bgv[b] = weight * profile[b] + offset
     // is subtracted from every output value of bin b after the scaling.
     const float* bgv;
+    int bitshift;  // DataParameters::bitshift for 8/16-bit samples: each sample >> 4 before the chain
 };
 
 template <int N_>
@@ -423,6 +424,21 @@ OPE_HD void phase_store_packed(int t, const uint32_t* words, uint32_t* specw) {
         if (p == N / 2 - 1)
             for (int e = 0; e < SPEC_PAD; ++e) specw[SPEC_PAD + N + e] = words[2 * k + 1];
     }
+}
+
+// DataParameters::bitshift as the reference's GPU path applies it
+// (inputToCufftComplex_and_bitshift, cuda_kernels.cu:45-63; the reference CPU
+// backend ignores the flag): every 8- or 16-bit sample shifted right by 4,
+// in place in the stage before the unpack, so every later step sees the
+// shifted integers.
+template <int N, int DT>
+OPE_HD void phase_bitshift(int t, unsigned char* stage) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    constexpr int T = Plan<N>::T;
+    constexpr int WORDS = 2 * N * (int)sizeof(raw_t) / 4;  // 32-bit words of the two rows
+    const uint32_t mask = DT == IN_U8 ? 0x0F0F0F0Fu : 0x0FFF0FFFu;
+    uint32_t* w = reinterpret_cast<uint32_t*>(stage);
+    for (int i = t; i < WORDS; i += T) w[i] = (w[i] >> 4) & mask;
 }
 
 // Rolling-average DC removal (cpu_kernels.tpp:56-82): x[i] -= mean of

@@ -349,3 +349,23 @@ def test_sinusoidal_scan_correction(cuda, with_bg):
     # last-bit difference in x (ulp up to 4e-6 for x < 64) moves the fraction,
     # so outputs agree to |f1 - f0| * 4e-6 rather than to the last bit
     assert np.allclose(got, want, rtol=0, atol=1e-5), np.abs(got - want).max()
+
+
+@pytest.mark.parametrize("dtype", [UINT8, UINT16])
+@pytest.mark.parametrize("dc", [False, True])
+def test_bitshift_equals_the_pre_shifted_input(cuda, dtype, dc):
+    """DataParameters::bitshift (the reference GPU path's rule: 8/16-bit samples
+    >> 4) gives every bit of the image of the input shifted on the host;
+    32-bit samples ignore the flag."""
+    spec = spec_for(1024, CUBIC, dtype=dtype, m=7, dc_removal=dc, dc_window=32)
+    raw = H.random_raw(spec, seed=4)
+    got = H.gpu_run(spec.with_(bitshift=True), raw)
+    want = H.gpu_run(spec, (raw >> 4).astype(raw.dtype))
+    assert np.array_equal(got, want)
+    assert not np.array_equal(got, H.gpu_run(spec, raw))
+
+
+def test_bitshift_ignored_for_32_bit_samples(cuda):
+    spec = spec_for(512, LINEAR, dtype=UINT32, m=4)
+    raw = H.random_raw(spec, seed=5)
+    assert np.array_equal(H.gpu_run(spec.with_(bitshift=True), raw), H.gpu_run(spec, raw))
