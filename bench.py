@@ -706,11 +706,12 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         try:
-            rate, dt, ascans = cpu_reference_run(1, 1, threads)
+            # a bounded sample: 20 B-scans per core (about 20 core-seconds of work)
+            rate, dt, ascans = cpu_reference_run(20, 2, threads)
             rate1, _, _ = cpu_reference_run(3, 1, 1)
             cpu_base = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                        "sample": f"{ascans} A-scans ({threads} reference CpuBackend instances x 1 B-scan of the "
-                                  f"workload); FFT = project shim (float32 radix-2), not FFTW",
+                        "sample": f"{ascans} A-scans in {dt:.1f} s ({threads} reference CpuBackend instances x "
+                                  f"20 B-scans of the workload); FFT = project shim (float32 radix-2), not FFTW",
                         "single_instance": {"value": rate1, "cores": 1,
                                             "sample": "3 B-scans through one CpuBackend (its one worker thread)"}}
         except Exception as e:  # the reference library was not built for this machine
