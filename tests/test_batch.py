@@ -206,3 +206,17 @@ def test_batch_rejects_what_it_cannot_run(cuda):
             b.set_tuning(4096, 4, 1)  # 4096 has one schedule
         with pytest.raises(capi.B200Error):
             b.set_tuning(2048, 0, 0)
+
+
+def test_bitshift_in_a_batch(cuda):
+    from octproengine_b200.batch import Batch
+    specs = [_spec(2048, 40, UINT16, CUBIC, HANN, 11).with_(bitshift=True),
+             _spec(1024, 17, UINT8, LANCZOS, GAUSS, 12).with_(bitshift=True),
+             _spec(1024, 9, UINT16, LINEAR, HANN, 13)]
+    bufs = _Bufs(specs, cuda, seed=60)
+    ref = bufs.single()
+    with Batch(bufs.items()) as b:
+        b.run(_stream())
+        got = bufs.outputs()
+    for g, r in zip(got, ref):
+        assert np.array_equal(g, r)
