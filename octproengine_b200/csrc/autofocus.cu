@@ -25,10 +25,9 @@ __device__ __forceinline__ int af_trunc(float v) {
     return (int)v;
 }
 
-__global__ void af_tables_kernel(int n, int interp, const float* __restrict__ params,
-                                 const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
-                                 float* lzdw, float* rmask, float2* wph) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void af_tables(int j, int n, int interp, const float* __restrict__ params,
+                                          const float* __restrict__ window, int2* lin, int2* cub, int* lzb,
+                                          float* rmask, float2* wph) {
     if (j >= n) return;
     // resampling position (processorconfiguration.cpp:438-459)
     const float s1 = (float)n - 1.0f;
@@ -56,7 +55,7 @@ __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ pa
         const int n0 = af_trunc(nx);
         int b = n0 < -9 ? -9 : (n0 > n + 7 ? n + 7 : n0);
         lzb[j] = b - 7 + SPEC_PAD;
-        // the 16 tap weights (and derivatives) come from af_lanczos_kernel
+        // the 16 tap weights (and derivatives) come from af_lanczos
     }
     // dispersion phase (processorconfiguration.cpp:461-482), window x (cos, sin)
     const float d0 = params[0];
@@ -73,8 +72,8 @@ __global__ void af_tables_kernel(int n, int interp, const float* __restrict__ pa
 
 // Lanczos-8 tap weights of every output sample, one thread per (tap, sample);
 // derivative weights only when the adjoint needs them.
-__global__ void af_lanczos_kernel(int n, const float* __restrict__ params, float* lzw, float* lzdw) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void af_lanczos(int i, int n, const float* __restrict__ params, float* lzw,
+                                           float* lzdw) {
     if (i >= 16 * n) return;
     const int k = i / n, j = i - k * n;
     const float s1 = (float)n - 1.0f;
@@ -91,6 +90,18 @@ __global__ void af_lanczos_kernel(int n, const float* __restrict__ params, float
     const float d = __fsub_rn(nx, (float)idx);
     lzw[i] = af_lanczos8(d);
     if (lzdw) lzdw[i] = af_lanczos8_deriv(d);
+}
+
+// Every table of one evaluation in one launch: blocks [0, tb) build the
+// per-sample tables, the blocks after them (Lanczos-8 only) the 16 tap
+// weights per sample.
+__global__ void af_prepare_kernel(int n, int interp, int tb, const float* __restrict__ params,
+                                  const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
+                                  float* lzdw, float* rmask, float2* wph) {
+    if ((int)blockIdx.x < tb)
+        af_tables(blockIdx.x * blockDim.x + threadIdx.x, n, interp, params, window, lin, cub, lzb, rmask, wph);
+    else
+        af_lanczos(((int)blockIdx.x - tb) * blockDim.x + threadIdx.x, n, params, lzw, lzdw);
 }
 
 // Deterministic block sum of `width` interleaved values per record over
@@ -211,15 +222,12 @@ int af_prepare(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float
     AF_CU(o, cudaSetDevice(o->device));
     if (build_tables) {
         const int threads = 256;
-        af_tables_kernel<<<(o->n + threads - 1) / threads, threads, 0, s>>>(o->n, o->interp, d_params, o->window,
-                                                                             o->lin, o->cub, o->lzb, o->lzw, o->lzdw,
-                                                                             o->rmask, o->wph);
+        const int tb = (o->n + threads - 1) / threads;
+        const int lb = o->interp == INTERP_LANCZOS ? (16 * o->n + threads - 1) / threads : 0;
+        af_prepare_kernel<<<tb + lb, threads, 0, s>>>(o->n, o->interp, tb, d_params, o->window, o->lin, o->cub,
+                                                      o->lzb, o->lzw, backward ? o->lzdw : nullptr, o->rmask,
+                                                      o->wph);
         AF_CU(o, cudaGetLastError());
-        if (o->interp == INTERP_LANCZOS) {
-            af_lanczos_kernel<<<(16 * o->n + threads - 1) / threads, threads, 0, s>>>(o->n, d_params, o->lzw,
-                                                                                     backward ? o->lzdw : nullptr);
-            AF_CU(o, cudaGetLastError());
-        }
         o->tables_params = d_params;
     }
     AfArgs a{};

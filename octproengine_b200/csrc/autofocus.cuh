@@ -71,14 +71,16 @@ __device__ __forceinline__ float af_lanczos8_deriv(float xf) {
     return static_cast<float>((ca - f1) / x * f2 + f1 * (cb - f2) / x);
 }
 
-// One thread per output sample j: resampling tables, window x phase factors
-// and the clamp mask from the device parameter vector. The polynomials are
+// The device tables of one evaluation, in one launch: one thread per output
+// sample j for the resampling tables, window x phase factors and the clamp
+// mask, then (Lanczos-8) one thread per (tap, sample) for the tap weights,
+// all from the device parameter vector. The polynomials are
 // evaluated as generateResamplingCurve / generateDispersionCurve do
 // (processorconfiguration.cpp:438-482): float Horner in j with the
 // coefficients divided by (N-1)^m, every operation rounded separately.
-__global__ void af_tables_kernel(int n, int interp, const float* __restrict__ params,
-                                 const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
-                                 float* lzdw, float* rmask, float2* wph);
+__global__ void af_prepare_kernel(int n, int interp, int tb, const float* __restrict__ params,
+                                  const float* __restrict__ window, int2* lin, int2* cub, int* lzb, float* lzw,
+                                  float* lzdw, float* rmask, float2* wph);
 
 // ------------------------------------------------------------ forward ----
 
