@@ -37,17 +37,47 @@ METRIC = "A-scans/s (2048-pt chain)"
 UNIT = "A-scans/s"
 WORKLOAD = ("2048 samples x 1024 A-scans x 64 B-scans uint16 per GPU, cubic resampling, Gaussian window, "
             "dispersion compensation, FPN removal, float32 log output")
+# The workload settings in plain numbers (ope::InterpolationMethod, ope::WindowType),
+# shared by both arms so that the reference arm needs nothing from the package.
+INTERP = {"linear": 0, "cubic": 1, "lanczos": 2}
+WINDOW_GAUSS, WINDOW_CENTER, WINDOW_FILL = 1, 0.5, 0.9
+DISPERSION_D2_D3 = (12.0, -6.0)
+GRAYSCALE_MIN, GRAYSCALE_MAX = 30.0, 110.0
+COUNTERS = os.path.join(ROOT, "profiles", "chain_kernel_n2048_cubic_u16.json")
+
+
+def synth_module():
+    """The seeded synthetic-spectrum generator (octproengine_b200/synth.py: numpy
+    and torch only, no native library), loaded as a standalone module so that
+    the reference arm imports nothing of the package."""
+    import importlib.util
+    name = "_ope_bench_synth"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "octproengine_b200", "synth.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def bench_config(world=1, bscans=None):
+    """The `config` object of the JSON line: identical in both arms."""
+    b = BSCANS if bscans is None else bscans
+    return {"workload": WORKLOAD, "signal_length": N, "ascans_per_bscan": ASCANS, "bscans_per_buffer": b,
+            "input": "uint16", "interpolation": "cubic", "window": "gauss", "dispersion": list(DISPERSION_D2_D3),
+            "fpn_removal": True, "output": "float32 log", "global_batch_ascans": world * ASCANS * b,
+            "l2": "inputs and outputs larger than L2", "parallelism": f"{world} independent buffers (no collective)"}
 
 
 def bench_spec(interp=None):
-    from octproengine_b200.chain import ChainSpec, CUBIC, GAUSS
-    from octproengine_b200 import synth
+    from octproengine_b200.chain import ChainSpec
+    synth = synth_module()
     return ChainSpec(signal_length=N, ascans_per_bscan=ASCANS, bscans_per_buffer=BSCANS, resampling=True,
-                     interpolation=CUBIC if interp is None else interp,
-                     resampling_coeffs=synth.linearising_coeffs(N), windowing=True, window_type=GAUSS,
-                     window_center=0.5, window_fill=0.9, dispersion=True,
-                     dispersion_coeffs=synth.compensating_coeffs(12.0, -6.0), fpn_removal=True,
-                     fpn_bscan_count=1, grayscale_min=30.0, grayscale_max=110.0)
+                     interpolation=INTERP["cubic"] if interp is None else interp,
+                     resampling_coeffs=synth.linearising_coeffs(N), windowing=True, window_type=WINDOW_GAUSS,
+                     window_center=WINDOW_CENTER, window_fill=WINDOW_FILL, dispersion=True,
+                     dispersion_coeffs=synth.compensating_coeffs(*DISPERSION_D2_D3), fpn_removal=True,
+                     fpn_bscan_count=1, grayscale_min=GRAYSCALE_MIN, grayscale_max=GRAYSCALE_MAX)
 
 
 def algorithmic_bytes_per_ascan(n=N, in_bytes=2):
@@ -55,18 +85,12 @@ def algorithmic_bytes_per_ascan(n=N, in_bytes=2):
 
 
 def algorithmic_flops_per_ascan(n=N):
-    """Floating-point operations one A-scan of the cubic chain needs: the
+    """Nominal floating-point operations of one A-scan of the cubic chain: the
     inverse DFT counted as 5 N log2 N (the conventional FFT count), the
-    reference's cubic Hermite formula 19 per sample (a: 4, b: 6, c: 1, pos^2: 1,
-    the Horner evaluation and + y1: 7), window 1 and phase 2 per sample, and per
-    output bin FPN 2, |X|^2 3, log 1 and the grayscale affine 4. 167 936 at
-    N = 2048."""
+    reference's cubic Hermite formula 19 per sample, window 1 and phase 2 per
+    sample, and per output bin FPN 2, |X|^2 3, log 1 and the grayscale affine
+    4. 167 936 at N = 2048. Context for the measured pipe counters only."""
     return 5 * n * int(np.log2(n)) + n * (19 + 3) + (n // 2) * (2 + 3 + 1 + 4)
-
-
-def fp32_peak_tflops(sm_mhz):
-    """Nominal FP32 peak: 148 SMs x 128 FP32 lanes x 2 (FMA) x SM clock."""
-    return 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
 
 
 def measured_peak():
@@ -78,14 +102,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic_per_ascan():
-    """DRAM bytes per A-scan of the chain kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "chain_kernel_n2048_cubic_u16.md")
-    if not os.path.exists(p):
+def kernel_counters():
+    """ncu counters of one chain-kernel launch (profiles/*.json, written from a
+    capture whose command the file names), or None."""
+    if not os.path.exists(COUNTERS):
         return None
-    with open(p) as f:
-        m = re.search(r"dram_bytes_per_ascan:\s*([0-9.]+)", f.read())
-    return float(m.group(1)) if m else None
+    with open(COUNTERS) as f:
+        return json.load(f)
 
 
 class ClockSampler:
@@ -149,23 +172,27 @@ def dist_setup():
     return rank_setup()
 
 
+def ref_params(lib, bscans: int, interp: str = "cubic"):
+    """Reference configuration of the benchmark workload (plain numbers)."""
+    synth = synth_module()
+    return lib.make_params(N, ASCANS, bscans, 2, resampling=True, interpolation=INTERP[interp],
+                           resampling_coeffs=synth.linearising_coeffs(N), windowing=True, window_type=WINDOW_GAUSS,
+                           window_center=WINDOW_CENTER, window_fill=WINDOW_FILL, dispersion=True,
+                           dispersion_coeffs=synth.compensating_coeffs(*DISPERSION_D2_D3), fpn_removal=True,
+                           grayscale_min=GRAYSCALE_MIN, grayscale_max=GRAYSCALE_MAX)
+
+
 def cpu_reference_run(steps: int, warmup: int, threads: int, bscans_per_thread: int = 1):
     """Times the reference CPU backend (oracle/_ref, FFT = project shim in
     float32 mode, not FFTW) on `threads` independent backends, one B-scan of
     the benchmark workload each per step."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import reflib
-    from octproengine_b200 import synth
-    spec = bench_spec()
+    synth = synth_module()
     if not reflib.available():
         reflib.build()
     reflib.set_fft_precision("f32")
-    r, w, cs = spec.curves()
-    p = reflib.make_params(N, ASCANS, bscans_per_thread, 2, resampling=True, interpolation=spec.interpolation,
-                           resampling_coeffs=spec.resampling_coeffs, windowing=True, window_type=spec.window_type,
-                           window_center=spec.window_center, window_fill=spec.window_fill, dispersion=True,
-                           dispersion_coeffs=spec.dispersion_coeffs, fpn_removal=True,
-                           grayscale_min=spec.grayscale_min, grayscale_max=spec.grayscale_max)
+    p = ref_params(reflib, bscans_per_thread)
     raw = synth.as_numpy(synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=bscans_per_thread,
                                                           seed=1)), "uint16")
     prof = np.zeros(N, np.float32)
@@ -191,7 +218,7 @@ def cpu_reference_run(steps: int, warmup: int, threads: int, bscans_per_thread: 
     return ascans / dt, dt, ascans
 
 
-def cuda_reference_run(steps: int, warmup: int, interp=None):
+def cuda_reference_run(steps: int, warmup: int, interp: str = "cubic"):
     """Times the reference CUDA backend (oracle/_ref/libope_cuda_ref.so: the
     reference's cuda_backend.cu + cuda_kernels.cu, cuFFT for the DFT, built with
     the reference's default flags) on the benchmark workload through its own
@@ -200,15 +227,10 @@ def cuda_reference_run(steps: int, warmup: int, interp=None):
     D2H, counted at its output callback. Its first frame determines the FPN
     profile (warm-up); timed frames subtract it."""
     from oracle import refcuda
-    from octproengine_b200 import synth
-    spec = bench_spec(interp)
+    synth = synth_module()
     if not refcuda.available():
         refcuda.build()
-    p = refcuda.make_params(N, ASCANS, BSCANS, 2, resampling=True, interpolation=spec.interpolation,
-                            resampling_coeffs=spec.resampling_coeffs, windowing=True, window_type=spec.window_type,
-                            window_center=spec.window_center, window_fill=spec.window_fill, dispersion=True,
-                            dispersion_coeffs=spec.dispersion_coeffs, fpn_removal=True,
-                            grayscale_min=spec.grayscale_min, grayscale_max=spec.grayscale_max)
+    p = ref_params(refcuda, BSCANS, interp)
     raw = synth.as_numpy(synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=BSCANS, seed=100,
                                                           background_ripple=True)), "uint16")
     be = refcuda.RefCudaBackend(p)
@@ -224,7 +246,11 @@ def cuda_reference_run(steps: int, warmup: int, interp=None):
 
 
 def run_reference(args):
-    world, rank, _ = dist_setup()
+    """The reference arm: the reference's own implementation of the path, with
+    nothing of this package loaded (plain numbers for the workload, the data
+    generator loaded as a standalone module, rank from the environment)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
@@ -232,7 +258,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": None, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"{threads} x 1 B-scan (1024 A-scans) per step"},
+        "config": bench_config(world),
     }
     if not args.no_cpu_baseline:
         try:
@@ -245,7 +271,9 @@ def run_reference(args):
             "value": rate, "ms_per_step": 1e3 * dt / args.steps,
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{ascans} A-scans: {threads} reference CpuBackend instances in parallel, "
-                                       f"1 B-scan each per step; FFT = project shim (float32 radix-2), not FFTW",
+                                       f"1 B-scan (1024 A-scans) each per step; FFT = project shim (float32 "
+                                       f"radix-2), not FFTW",
+                             "sample_ascans_per_step": threads * ASCANS,
                              "single_instance": {"value": rate1, "cores": 1,
                                                  "sample": "3 B-scans through one CpuBackend (its one worker "
                                                            "thread)"}},
@@ -253,10 +281,9 @@ def run_reference(args):
         })
     if not args.no_cuda_reference:
         # the reference's own GPU path on the same workload, end to end through its API
-        from octproengine_b200.chain import LANCZOS
         try:
             cb = cuda_reference_run(args.steps, args.warmup)
-            cb["variants"] = {"lanczos8": cuda_reference_run(max(3, args.steps // 2), args.warmup, LANCZOS)}
+            cb["variants"] = {"lanczos8": cuda_reference_run(max(3, args.steps // 2), args.warmup, "lanczos")}
             cb["kind"] = ("reference CudaBackend (cuda_backend.cu + cuda_kernels.cu, cuFFT), --use_fast_math, "
                           "sm_100; end to end: registered host ring, H2D + chain + D2H per buffer")
             line["cuda_backend"] = cb
@@ -565,8 +592,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    from octproengine_b200.chain import LINEAR, CUBIC
-    interp = {"linear": LINEAR, "cubic": CUBIC, "lanczos": LANCZOS}[args.interp]
+    interp = INTERP[args.interp]
     spec = bench_spec(interp).with_(device=local, bscans_per_buffer=BSCANS)
     M = spec.num_ascans
     x = synth.generate(synth.SynthParams(n=N, ascans=ASCANS, bscans=BSCANS, seed=100 + rank,
@@ -622,7 +648,7 @@ def run_ours(args):
     bytes_launch = M * algorithmic_bytes_per_ascan()
     achieved = bytes_launch / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    tpa = profile_traffic_per_ascan()
+    counters = kernel_counters()
 
     variants = {}
     if args.kernel_only:
@@ -723,21 +749,29 @@ def run_ours(args):
     if rank != 0:
         return 0
     clocks = clk.summary()
-    fp32_achieved = M * algorithmic_flops_per_ascan() / (kernel_ms / 1e3) / 1e12
-    fp32_peak = fp32_peak_tflops(clocks.get("sm_mhz"))
+    traffic = None
+    pipes = None
+    if counters:
+        # DRAM bytes of one captured launch, scaled to this launch by A-scan count
+        per_ascan = (counters["dram_bytes_read"] + counters["dram_bytes_write"]) / counters["ascans"]
+        traffic = per_ascan * M
+        pipes = {k: counters[k] for k in ("fma_pipe_active_pct", "issue_active_pct", "warps_active_pct",
+                                          "thread_inst_per_ascan", "l1_data_pipe_pct") if k in counters}
+        pipes.update({"flops_per_ascan_nominal": algorithmic_flops_per_ascan(),
+                      "source": f"ncu, one launch over {counters['ascans']} A-scans: {counters['command']}"})
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "global_batch_ascans": world * M, "l2": "inputs and outputs larger than L2",
-                   "parallelism": f"{world} independent buffers (no collective)"},
+        "config": bench_config(world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (tpa * M) if tpa else None,
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_note": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch over "
+                                      f"{counters['ascans']} A-scans, scaled to {M} by A-scan count; writes "
+                                      f"still held in L2 when the kernel ends are not counted") if counters else None,
                      "algorithmic_bytes": bytes_launch},
-        "roofline_fp32": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                          "frac": fp32_achieved / fp32_peak, "flops_per_ascan": algorithmic_flops_per_ascan(),
-                          "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x 2 (FMA) x median sampled SM clock"},
+        # the chain's other roof: the FP32 pipe, as ncu counted it for one launch
+        "fp32_pipe": pipes,
         # end to end through the reference-facing streaming path (the frame ring that
         # process(IOBuffer&) feeds); the one-call synchronous path beside it
         "e2e": e2e_stream,

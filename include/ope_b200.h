@@ -181,10 +181,15 @@ OPE_B200_API int ope_b200_get_fpn_profile(ope_b200_ctx* ctx, float* out, size_t 
  * (num_ascans A-scans, at least that many) and writes N/2 interleaved
  * (re, im) float pairs to d_profile (8-byte aligned). Asynchronous on
  * `stream`; the context's own FPN state is not changed. Limits: signal length
- * up to 4096 (OPE_B200_E_UNSUPPORTED beyond). The first call on a device looks
- * up the array's device address; make that first call before any stream
- * capture. All calls share the one array: calls that overlap on the GPU race
- * and corrupt each other's results. */
+ * up to 4096 (OPE_B200_E_UNSUPPORTED beyond). Every call looks up the array's
+ * device address in the current context (no cached address survives a device
+ * reset); make the first call on a device before any stream capture. All calls
+ * share the one array: calls that overlap on the GPU race and corrupt each
+ * other's results. The call blocks the host in one case: when a curve or the
+ * configuration changed since the last processing call, it first rebuilds the
+ * context's device tables (a synchronous upload). A real-time loop avoids that
+ * stall by processing one buffer (or calling this once) after every curve or
+ * configuration change, before it enters the loop. */
 OPE_B200_API int ope_b200_determine_fpn_noalloc(ope_b200_ctx* ctx, const void* d_in, int64_t num_ascans,
                                                 float* d_profile, void* stream);
 

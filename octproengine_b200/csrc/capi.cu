@@ -983,21 +983,16 @@ constexpr size_t kNoAllocAcc = static_cast<size_t>(FPN_SEGMENTS) * (kNoAllocMaxN
 // 3.4 MiB per GPU that loads the library, held until the process exits.
 static __device__ __align__(256) double g_fpn_noalloc_scratch[kNoAllocPartial + kNoAllocAcc];
 
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[64] = {nullptr};
-
-// Device address of the scratch array on the current device (`dev`). In host
+// Device address of the scratch array in the current device's context. In host
 // code the array's name is only a host-side stand-in, never a device address.
-cudaError_t noalloc_scratch(int dev, double** out) {
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_fpn_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_ptr[dev] = static_cast<double*>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+// Looked up on every call (cheap once the module is loaded): an address cached
+// across calls would go stale if the host application reset the device and a
+// new primary context reloaded the module elsewhere.
+cudaError_t noalloc_scratch(double** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fpn_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<double*>(p);
     return cudaSuccess;
 }
 
@@ -1023,7 +1018,7 @@ int ope_b200_determine_fpn_noalloc(ope_b200_ctx* c, const void* d_in, int64_t nu
         return fail(c, OPE_B200_E_INVALID, "buffer holds fewer A-scans than fpnBscanCount * ascansPerBscan");
     OPE_CU(c, cudaSetDevice(c->device));
     double* scratch = nullptr;
-    OPE_CU(c, noalloc_scratch(c->device, &scratch));
+    OPE_CU(c, noalloc_scratch(&scratch));
     if (c->tables_dirty) {
         int rc = rebuild_tables(c);
         if (rc != OPE_B200_OK) return rc;

@@ -25,12 +25,12 @@ _lib: Optional[ctypes.CDLL] = None
 
 
 def build(force: bool = False) -> bool:
-    """Compile the reference CUDA backend if the reference tree is present."""
-    if os.path.exists(LIB_PATH) and not force:
-        return True
-    if not os.path.isdir(REFERENCE_TREE):
-        return False
-    subprocess.run(["make", "-C", HERE, f"REF={REFERENCE_TREE}", "cuda"], check=True, stdout=subprocess.DEVNULL)
+    """Compile (or bring up to date) the reference CUDA backend when the
+    reference tree is named by OPE_REFERENCE_TREE; otherwise use the prebuilt
+    library."""
+    if REFERENCE_TREE and os.path.isdir(REFERENCE_TREE):
+        subprocess.run(["make", "-C", HERE, f"REF={REFERENCE_TREE}", "cuda"] + (["-B"] if force else []),
+                       check=True, stdout=subprocess.DEVNULL)
     return os.path.exists(LIB_PATH)
 
 

@@ -16,7 +16,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libope_cpu_ref.so")
-REFERENCE_TREE = "/root/reference"
+# Source tree of the reference (read-only), named by the environment; there is
+# no default. Without it the prebuilt _ref/ libraries are used as they are.
+REFERENCE_TREE = os.environ.get("OPE_REFERENCE_TREE", "")
 
 
 class RefParams(ctypes.Structure):
@@ -52,13 +54,11 @@ class RefParams(ctypes.Structure):
 
 
 def build(force: bool = False) -> bool:
-    """Compile the reference oracle if the reference tree is present."""
-    if os.path.exists(LIB_PATH) and not force:
-        return True
-    if not os.path.isdir(REFERENCE_TREE):
-        return False
-    subprocess.run(["make", "-C", HERE, f"REF={REFERENCE_TREE}"], check=True,
-                   stdout=subprocess.DEVNULL)
+    """Compile (or bring up to date) the reference oracle when the reference
+    tree is named by OPE_REFERENCE_TREE; otherwise use the prebuilt library."""
+    if REFERENCE_TREE and os.path.isdir(REFERENCE_TREE):
+        subprocess.run(["make", "-C", HERE, f"REF={REFERENCE_TREE}"] + (["-B"] if force else []), check=True,
+                       stdout=subprocess.DEVNULL)
     return os.path.exists(LIB_PATH)
 
 

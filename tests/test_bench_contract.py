@@ -26,3 +26,22 @@ def test_reference_arm_prints_one_json_line_without_a_gpu(reflib):
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert cb["single_instance"]["cores"] == 1 and cb["single_instance"]["value"] > 0
     assert "unavailable" in d["cuda_backend"]
+
+
+def test_reference_arm_loads_nothing_of_the_package(reflib):
+    """The reference arm times the reference alone: after a full run of it, no
+    module of octproengine_b200 is imported and libope_b200.so is not mapped,
+    and its `config` object is the one the product arm prints."""
+    code = ("import sys, runpy\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '3', '--no-cuda-reference']\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('PKG', any(m == 'octproengine_b200' or m.startswith('octproengine_b200.') for m in sys.modules))\n"
+            "print('SO', 'libope_b200' in maps, 'libope_host' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PKG False" in r.stdout and "SO False False" in r.stdout, r.stdout[-500:]
+    line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == json.loads(json.dumps(bench.bench_config(1)))

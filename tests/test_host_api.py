@@ -242,7 +242,7 @@ def test_host_library_exports():
     ctypes.CDLL(B.HOST_LIB)
 
 
-REF_EXAMPLE = "/root/reference/examples/example_basic.cpp"
+REF_EXAMPLE = os.path.join(os.environ.get("OPE_REFERENCE_TREE", "/nonexistent"), "examples", "example_basic.cpp")
 
 
 @pytest.mark.skipif(not os.path.exists(REF_EXAMPLE), reason="reference sources not present")

@@ -18,20 +18,24 @@ from octproengine_b200.chain import ChainSpec, open_context, CUBIC, HANN
 pytestmark = pytest.mark.gpu
 
 
-def _spec(n=2048):
-    return ChainSpec(signal_length=n, ascans_per_bscan=256, bscans_per_buffer=2, resampling=True,
+def _spec(n=2048, ascans=256):
+    return ChainSpec(signal_length=n, ascans_per_bscan=ascans, bscans_per_buffer=2, resampling=True,
                      interpolation=CUBIC, resampling_coeffs=(0.5, float(n), -100.0, 50.0), windowing=True,
                      window_type=HANN, window_center=0.5, window_fill=0.9, dispersion=True,
                      dispersion_coeffs=(0.0, 0.0, 1.0, -3.0), fpn_removal=True, fpn_bscan_count=1,
                      grayscale_min=20.0, grayscale_max=110.0)
 
 
-def test_noalloc_fpn_matches_allocating_path_twice(cuda):
+@pytest.mark.parametrize("n,ascans", [(1024, 256), (2048, 256), (4096, 256), (2048, 64)])
+def test_noalloc_fpn_matches_allocating_path_twice(cuda, n, ascans):
     """Two calls in a row through the C ABI each give the profile of the
     allocating path (request + process) within the FPN test tolerance; the
-    second call proves the shared scratch is cleared between calls."""
+    second call proves the shared scratch is cleared between calls. N = 4096
+    is the largest length the static scratch serves; 64 A-scans per
+    determination (8 per FPN segment) run one CTA per segment, 256 run the
+    full 8."""
     import torch
-    spec = _spec()
+    spec = _spec(n, ascans)
     m, half = spec.num_ascans, spec.signal_length // 2
     raw = H.random_raw(spec, seed=77)
     d_in = torch.from_numpy(raw.view(np.uint8).reshape(-1).copy()).to("cuda:0")
