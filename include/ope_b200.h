@@ -90,7 +90,11 @@ typedef struct ope_b200_config {
                                   mean is subtracted before the chain and its float64
                                   response added back after the DFT (same quantity,
                                   lower float32 error; ignored with DC removal on) */
-    int32_t reserved[8];
+    int32_t dc_reference_order; /* rolling-average DC removal: 0 (default) = exact integer
+                                  window sums; 1 = the reference CPU backend's sequential
+                                  float prefix sum (rollingAverageDCRemoval,
+                                  cpu_kernels.tpp:56-82), bit for bit */
+    int32_t reserved[7];
 } ope_b200_config;
 
 typedef struct ope_b200_ctx ope_b200_ctx;
@@ -369,6 +373,12 @@ OPE_B200_API int ope_b200_op_background_subtraction(const float* input, const fl
  * kernel then records a status that ope_b200_synchronize / process_host
  * report, and the context stays usable. */
 OPE_B200_API int ope_b200_test_inject_copy_stall(ope_b200_ctx* ctx, uint32_t timeout_us);
+/* Test hook, no reference counterpart: the next launch of this context issues
+ * its first input copies as usual but treats each CTA's first wait as run out,
+ * so every CTA takes the timeout path with its copy still in flight or just
+ * landed: it waits that copy out (a second bound) before returning and records
+ * the timeout status alone; the context stays usable. */
+OPE_B200_API int ope_b200_test_inject_wait_abort(ope_b200_ctx* ctx);
 
 /* ABI version and build information. */
 OPE_B200_API int ope_b200_abi_version(void);

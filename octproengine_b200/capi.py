@@ -72,7 +72,8 @@ class Config(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("num_input_buffers", ctypes.c_int32),
         ("dc_split", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 8),
+        ("dc_reference_order", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 
@@ -94,6 +95,7 @@ SIGNATURES = {
     "ope_b200_process_host": (ctypes.c_int, [_P, _P, _P]),
     "ope_b200_process_bins_device": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "ope_b200_test_inject_copy_stall": (ctypes.c_int, [_P, ctypes.c_uint32]),
+    "ope_b200_test_inject_wait_abort": (ctypes.c_int, [_P]),
     "ope_b200_ring_depth": (ctypes.c_int, [_P]),
     "ope_b200_host_register": (ctypes.c_int, [_P, _SZ]),
     "ope_b200_host_unregister": (ctypes.c_int, [_P]),
@@ -280,6 +282,9 @@ class Context:
 
     def inject_copy_stall(self, timeout_us: int) -> None:
         self.check(lib().ope_b200_test_inject_copy_stall(self.h, int(timeout_us)))
+
+    def inject_wait_abort(self) -> None:
+        self.check(lib().ope_b200_test_inject_wait_abort(self.h))
 
     def process_host(self, raw: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
         n = self.cfg.signal_length

@@ -55,6 +55,9 @@ class ChainSpec:
     float32_as_uint32: bool = False
     bitshift: bool = False  # 8/16-bit samples >> 4 before the chain
     dc_split: bool = True
+    # rolling-average DC removal in the reference CPU backend's order (its
+    # sequential float prefix sum) instead of exact integer window sums
+    dc_reference_order: bool = False
     device: int = 0
     num_input_buffers: int = 2  # depth of the host frame ring
     # custom curves (used instead of the generated ones when given)
@@ -97,6 +100,7 @@ class ChainSpec:
         c.float32_as_uint32 = int(self.float32_as_uint32)
         c.bitshift = int(self.bitshift)
         c.dc_split = int(self.dc_split)
+        c.dc_reference_order = int(self.dc_reference_order)
         c.device = int(self.device)
         c.num_input_buffers = int(self.num_input_buffers)
         return c

@@ -119,6 +119,7 @@ struct ope_b200_ctx {
 
     // test hook: next launch skips its first bulk copy and waits at most this long
     unsigned long long inject_stall_ns = 0;
+    bool inject_wait_abort = false;
 
     // streaming ring (ope_b200_submit / wait / release)
     struct RingSlot {
@@ -286,6 +287,7 @@ static ChainArgs make_args(ope_b200_ctx* c, const void* d_in, float* d_out, long
     a.wph = s.wph;
     a.fpn = fpn;
     a.dc_window = c->cfg.dc_removal_enabled ? c->cfg.dc_window : 0;
+    a.dc_ref_order = c->cfg.dc_reference_order ? 1 : 0;
     const auto& cf = c->cfg;
     scaling_constants(cf.log_scaling != 0, cf.grayscale_min, cf.grayscale_max, cf.addend, cf.multiplicator, c->n, a);
     a.flip = c->cfg.bscan_flip ? 1 : 0;
@@ -584,6 +586,10 @@ static int process_locked(ope_b200_ctx* c, const void* d_in, void* d_out, long l
         a.timeout_ns = c->inject_stall_ns;
         c->inject_stall_ns = 0;
     }
+    if (c->inject_wait_abort) {
+        a.debug_abort_first_wait = 1;
+        c->inject_wait_abort = false;
+    }
     cudaError_t e = launch_chain(c->n, c->in_kind, c->interp, a, s, 0, nullptr);
     if (e != cudaSuccess) return cuda_fail(c, e, "chain launch");
     OPE_CU(c, cudaEventRecord(c->slot[c->active].last_use, s));
@@ -622,6 +628,13 @@ int ope_b200_test_inject_copy_stall(ope_b200_ctx* c, uint32_t timeout_us) {
     if (!c) return OPE_B200_E_INVALID;
     std::lock_guard<std::mutex> lk(c->mu);
     c->inject_stall_ns = static_cast<unsigned long long>(timeout_us ? timeout_us : 1) * 1000ull;
+    return OPE_B200_OK;
+}
+
+int ope_b200_test_inject_wait_abort(ope_b200_ctx* c) {
+    if (!c) return OPE_B200_E_INVALID;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->inject_wait_abort = true;
     return OPE_B200_OK;
 }
 

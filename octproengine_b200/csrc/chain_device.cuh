@@ -229,7 +229,8 @@ __device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, con
 // Raw rows are staged by cp.async.bulk into one shared-memory stage: the copy
 // of the next pair is issued as soon as this pair's rows are unpacked, so it
 // overlaps the resampling, the DFT and the epilogue. Every wait is bounded
-// (a.timeout_ns) and a timeout sets STATUS_MBAR_TIMEOUT and returns.
+// (a.timeout_ns); a timeout sets STATUS_MBAR_TIMEOUT and returns once the copy
+// in flight has landed (STATUS_COPY_PENDING if that too runs out).
 // `tm` is the team running the pairs (the CTA, or a named-barrier sub-team
 // whose shared-memory region starts at smem); S selects the radix schedule.
 template <int N, int DT, int INTERP, int S, class Team, class Sink>
@@ -272,16 +273,29 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
     };
 
     long long item = p0;
-    if (t == 0 && item < p_end && !a.debug_skip_first_copy) issue(item);
+    // thread 0: whether a copy was issued for the phase being waited on
+    bool issued = false;
+    if (t == 0 && item < p_end && !a.debug_skip_first_copy) {
+        issue(item);
+        issued = true;
+    }
 
     for (int it = 0; item < p_end; item += step, ++it) {
         const long long nxt = item + step;
-        if (!mbar_wait_bounded(&mbar[0], it & 1, a.timeout_ns)) *abort_flag = 1;
+        const bool ok = (it == 0 && a.debug_abort_first_wait) ? false
+                                                               : mbar_wait_bounded(&mbar[0], it & 1, a.timeout_ns);
+        if (!ok) *abort_flag = 1;
         tm.sync();
         if (*abort_flag) {
-            // nothing else is in flight: the next copy is only issued after a
-            // successful wait
-            if (t == 0 && a.status) atomicOr(a.status, STATUS_MBAR_TIMEOUT);
+            // A copy issued for this phase may still be writing into this CTA's
+            // shared memory and counting against its mbarrier: thread 0 waits it
+            // out (a second bound) before the CTA returns, and says so in the
+            // status if even that runs out.
+            if (t == 0) {
+                int st = STATUS_MBAR_TIMEOUT;
+                if (issued && !mbar_wait_bounded(&mbar[0], it & 1, a.timeout_ns)) st |= STATUS_COPY_PENDING;
+                if (a.status) atomicOr(a.status, st);
+            }
             return;
         }
         const unsigned char* stage = stages;
@@ -309,6 +323,10 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
                 cbias = add2(cbias, dc);  // 2^23 + c, exact for c < 2^23
             }
             phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
+        } else if (a.dc_window > 0 && a.dc_ref_order) {
+            phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
+            tm.sync();
+            phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);
         } else if (a.dc_window > 0) {
             sum_t ta, tb;
             phase_dc_local<N, DT>(t, stage, &ta, &tb);
@@ -328,7 +346,10 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
             phase_unpack<N, DT>(t, stage, spec);
         }
         tm.sync();
-        if (t == 0 && nxt < p_end) issue(nxt);  // every thread is done with the stage
+        if (t == 0) {  // every thread is done with the stage
+            issued = nxt < p_end;
+            if (issued) issue(nxt);
+        }
 
         // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];

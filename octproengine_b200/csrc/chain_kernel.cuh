@@ -46,7 +46,8 @@ enum InterpKind : int { INTERP_NONE = 0, INTERP_LINEAR = 1, INTERP_CUBIC = 2, IN
 constexpr int SPEC_PAD = 16;
 
 // Device status word bits.
-constexpr int STATUS_MBAR_TIMEOUT = 1;
+constexpr int STATUS_MBAR_TIMEOUT = 1;  // a bounded wait for an input copy ran out
+constexpr int STATUS_COPY_PENDING = 2;  // ... and the copy had still not landed after a second bound
 
 struct ChainArgs {
     const void* in;      // m rows x n samples
@@ -84,6 +85,8 @@ struct ChainArgs {
     // is subtracted from every output value of bin b after the scaling.
     const float* bgv;
     int bitshift;  // DataParameters::bitshift for 8/16-bit samples: each sample >> 4 before the chain
+    int debug_abort_first_wait;  // test hook: treat the first wait as run out although its copy was issued
+    int dc_ref_order;  // rolling-average DC removal with the reference's sequential float prefix sum
 };
 
 template <int N_>
@@ -540,13 +543,47 @@ OPE_HD void phase_dc_prefix(int t, const unsigned char* stage, typename InTraits
     }
 }
 
+// Rolling-average DC removal in the reference's own order
+// (rollingAverageDCRemoval, cpu_kernels.tpp:56-82): one sequential float
+// prefix sum per A-scan, cs[i+1] = cs[i] + x[i], each addition rounded. The
+// chain of additions is serial, so threads 0 and 1 run the two rows' sums
+// (row t) while the team waits; entry i of row r lives at pfx_idx(2*i + r).
+template <int DT>
+OPE_HD float sample_as_float(const unsigned char* stage, int n, int row, int i) {
+    using raw_t = typename InTraits<DT>::raw_t;
+    const raw_t x = reinterpret_cast<const raw_t*>(stage)[row * n + i];
+    if (DT == IN_U32) {
+#if defined(__CUDA_ARCH__)
+        return __uint2float_rn((unsigned)x);
+#else
+        return (float)(unsigned)x;
+#endif
+    }
+    return (float)x;
+}
+
+template <int N, int DT>
+OPE_HD void phase_dc_ref_scan(int t, const unsigned char* stage, float* pf) {
+    if (t > 1) return;
+    float s = 0.0f;
+    pf[pfx_idx(t)] = 0.0f;
+#pragma unroll 8
+    for (int i = 0; i < N; ++i) {
+        s = fadd_rn(s, sample_as_float<DT>(stage, N, t, i));
+        OPE_SMEM_CHECK(pfx_idx(2 * (i + 1) + t) < pfx_idx(2 * (N + 1)));
+        pf[pfx_idx(2 * (i + 1) + t)] = s;
+    }
+}
+
 // Step C: subtract the window means and write the spectrum pairs. A window of
 // a power-of-two count (the interior, when 2W is one: W = 64 by default) is
 // divided by multiplying with its exact reciprocal, which equals the correctly
 // rounded quotient; other counts use the correctly rounded division.
-template <int N, int DT>
-OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InTraits<DT>::sum_t* pfx,
-                           int W, float2* spec) {
+// REF = false: exact window sums from the integer prefix sums of
+// phase_dc_prefix; REF = true: the reference's float difference of two entries
+// of the sequential float prefix sum (phase_dc_ref_scan).
+template <int N, int DT, bool REF = false>
+OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const void* pfx_v, int W, float2* spec) {
     using sum_t = typename InTraits<DT>::sum_t;
     constexpr int T = Plan<N>::T;
     const int full = 2 * W;
@@ -561,21 +598,29 @@ OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const typename InT
             int i = 8 * c + k;
             int start = (i >= W - 1) ? i - (W - 1) : 0;
             int end = (i + W < N - 1) ? i + W : N - 1;
-            sum_t sa = pfx[pfx_idx(2 * (end + 1))] - pfx[pfx_idx(2 * start)];
-            sum_t sb = pfx[pfx_idx(2 * (end + 1) + 1)] - pfx[pfx_idx(2 * start + 1)];
+            float fa, fb;
+            if constexpr (REF) {
+                const float* pf = static_cast<const float*>(pfx_v);
+                fa = fsub_rn(pf[pfx_idx(2 * (end + 1))], pf[pfx_idx(2 * start)]);
+                fb = fsub_rn(pf[pfx_idx(2 * (end + 1) + 1)], pf[pfx_idx(2 * start + 1)]);
+            } else {
+                const sum_t* pfx = static_cast<const sum_t*>(pfx_v);
+                fa = (float)(pfx[pfx_idx(2 * (end + 1))] - pfx[pfx_idx(2 * start)]);
+                fb = (float)(pfx[pfx_idx(2 * (end + 1) + 1)] - pfx[pfx_idx(2 * start + 1)]);
+            }
             const int n = end - start + 1;
             float ma, mb;
             if (full_pow2 && n == full) {
-                ma = (float)sa * full_inv;
-                mb = (float)sb * full_inv;
+                ma = fmul_rn(fa, full_inv);
+                mb = fmul_rn(fb, full_inv);
             } else {
                 float cnt = (float)n;
 #if defined(__CUDA_ARCH__)
-                ma = __fdiv_rn((float)sa, cnt);
-                mb = __fdiv_rn((float)sb, cnt);
+                ma = __fdiv_rn(fa, cnt);
+                mb = __fdiv_rn(fb, cnt);
 #else
-                ma = (float)sa / cnt;
-                mb = (float)sb / cnt;
+                ma = fa / cnt;
+                mb = fb / cnt;
 #endif
             }
             v[k] = sub2(v[k], make_float2(ma, mb));

@@ -26,7 +26,7 @@ namespace {
 
 constexpr int kWaitMs = 120000;  // host-side bound on any single frame wait
 
-ope_b200_config to_c(const ProcessorConfiguration& c, int depth) {
+ope_b200_config to_c(const ProcessorConfiguration& c, int depth, bool dc_reference_order) {
     ope_b200_config o;
     ope_b200_config_default(&o);
     o.signal_length = c.dataParams.signalLength;
@@ -55,6 +55,7 @@ ope_b200_config to_c(const ProcessorConfiguration& c, int depth) {
     o.bscan_flip = p.bscanFlip;
     o.sinusoidal_correction = p.sinusoidalScanCorrection;
     o.num_input_buffers = depth;
+    o.dc_reference_order = dc_reference_order ? 1 : 0;
     return o;
 }
 
@@ -64,6 +65,7 @@ struct B200Backend::Impl {
     ope_b200_ctx* ctx = nullptr;
     ProcessorConfiguration config;
     int depth = 0;
+    bool dc_reference_order = true;
     size_t in_bytes = 0, out_bytes = 0;
 
     std::mutex cb_mu;
@@ -150,13 +152,15 @@ B200Backend::B200Backend() : impl(std::make_unique<Impl>()) {}
 
 B200Backend::~B200Backend() { cleanup(); }
 
+void B200Backend::setRollingAverageReferenceOrder(bool on) { impl->dc_reference_order = on; }
+
 void B200Backend::initialize(const ProcessorConfiguration& config) {
     cleanup();
     auto& m = *impl;
     m.config = config;
     int nb = config.processingParams.nBuffers;
     m.depth = nb < 2 ? 2 : (nb > 4 ? 4 : nb);
-    const ope_b200_config c = to_c(config, m.depth);
+    const ope_b200_config c = to_c(config, m.depth, m.dc_reference_order);
     m.check(ope_b200_create(&c, &m.ctx), "B200 backend initialization");
     const size_t samples = static_cast<size_t>(config.dataParams.signalLength) * config.dataParams.ascansPerBscan *
                            config.dataParams.bscansPerBuffer;
@@ -230,7 +234,7 @@ void B200Backend::updateConfig(const ProcessorConfiguration& config) {
     auto& m = *impl;
     m.config = config;
     if (!m.ctx) return;
-    const ope_b200_config c = to_c(config, m.depth);
+    const ope_b200_config c = to_c(config, m.depth, m.dc_reference_order);
     m.check(ope_b200_update_config(m.ctx, &c), "updateConfig");
 }
 

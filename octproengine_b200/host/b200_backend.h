@@ -67,6 +67,13 @@ public:
                                                         float weight, float offset, int lineWidth,
                                                         int samples) override;
 
+    // Rolling-average DC removal. true (the default): the reference CPU
+    // backend's sequential float prefix sum, so a frame with background
+    // removal on equals that backend's output bit for bit up to the DFT;
+    // false: exact integer window sums (the exact mean of each window).
+    // Takes effect at the next initialize() or updateConfig().
+    void setRollingAverageReferenceOrder(bool on);
+
 private:
     struct Impl;
     std::unique_ptr<Impl> impl;

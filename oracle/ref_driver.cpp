@@ -12,6 +12,7 @@
 //  * one blocking "process a frame" call: getNextAvailableInputBuffer, copy in,
 //    process, wait for the output callback, copy out (processor.cpp:348-365).
 #include "backends/cpu/cpu_backend.h"
+#include "backends/cpu/cpu_kernels.h"
 #include "processorconfiguration.h"
 #include "iobuffer.h"
 #include "types.h"
@@ -325,6 +326,16 @@ int ope_ref_ifft_magnitude(const float* in, int n, float* out) {
     ope::CpuBackend* be = lowlevel_backend(n);
     std::vector<float> v = be->ifft(in, n, n);
     std::memcpy(out, v.data(), v.size() * sizeof(float));
+    return 0;
+}
+
+// The reference's rolling-average DC removal of one line (its float prefix
+// sum; the CpuBackend's low-level rollingAverageBackgroundRemoval does not run it).
+int ope_ref_rolling_dc(const float* in, int n, int window, float* out) {
+    std::vector<std::complex<float>> v(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) v[i] = std::complex<float>(in[i], 0.0f);
+    ope::cpu_kernels::rollingAverageDCRemoval(v, static_cast<size_t>(window));
+    for (int i = 0; i < n; ++i) out[i] = v[i].real();
     return 0;
 }
 

@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
         L.ope_ref_min_var_mean.argtypes = [fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp]
         L.ope_ref_ifft_magnitude.argtypes = [fp, ctypes.c_int, fp]
         L.ope_ref_fft_shim_precision.argtypes = [ctypes.c_int]
+        L.ope_ref_rolling_dc.argtypes = [fp, ctypes.c_int, ctypes.c_int, fp]
         L.ope_ref_fft_shim_precision.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -202,11 +203,28 @@ class RefBackend:
             pass
 
 
+def convert_input(raw: np.ndarray, dtype: int) -> np.ndarray:
+    """The reference's convertInput of one line of raw samples (ope::DataType dtype)."""
+    raw = np.ascontiguousarray(raw)
+    out = np.zeros(raw.size, np.float32)
+    lib().ope_ref_convert_input(raw.ctypes.data, int(dtype), raw.size, _fp(out))
+    return out
+
+
 def klinearization(x: np.ndarray, curve: np.ndarray, method: int) -> np.ndarray:
     x = np.ascontiguousarray(x, np.float32)
     c = np.ascontiguousarray(curve, np.float32)
     out = np.zeros(x.size, np.float32)
     lib().ope_ref_klinearization(_fp(x), _fp(c), method, x.size, _fp(out))
+    return out
+
+
+def rolling_dc(x: np.ndarray, window: int) -> np.ndarray:
+    """The reference's rollingAverageDCRemoval on each row of x (float32)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    for i in range(x.shape[0]):
+        lib().ope_ref_rolling_dc(_fp(x[i]), x.shape[1], int(window), _fp(out[i]))
     return out
 
 

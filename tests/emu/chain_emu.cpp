@@ -32,6 +32,7 @@ struct EmuArgs {
     float gmin, gmax, addend, mult;
     int flip, ascans_per_bscan, bscans;
     int dc_split;
+    int dc_ref_order;
 };
 }
 
@@ -120,6 +121,10 @@ int emu_run(const EmuArgs& e, int what, float* out) {
             }
             dc = make_float2(split_level((double)ta, N, DT != IN_F32), split_level((double)tb, N, DT != IN_F32));
             for (int t = 0; t < T; ++t) phase_split_store<N>(t, vals[t].data(), dc, spec);
+        } else if (e.dc_window > 0 && e.dc_ref_order) {
+            float* pf = reinterpret_cast<float*>(pfx);
+            for (int t = 0; t < T; ++t) phase_dc_ref_scan<N, DT>(t, stage.data(), pf);
+            for (int t = 0; t < T; ++t) phase_dc_apply<N, DT, true>(t, stage.data(), pf, e.dc_window, spec);
         } else if (e.dc_window > 0) {
             std::vector<sum_t> ta(T), tb(T);
             for (int t = 0; t < T; ++t) phase_dc_local<N, DT>(t, stage.data(), &ta[t], &tb[t]);

@@ -8,7 +8,7 @@ curves and outputs as .npz: ``out`` with the shim's DFT evaluated in float64,
 kernels are then checked against these files on machines without the
 reference tree.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]   # all cases, or the named ones
 """
 from __future__ import annotations
 
@@ -22,6 +22,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import reflib  # noqa: E402
+from octproengine_b200 import synth  # noqa: E402  (the benchmark's seeded generator; numpy + torch)
+
+_LIN2048 = synth.linearising_coeffs(2048)
+_DISP = synth.compensating_coeffs(12.0, -6.0)
 
 # (name, params for reflib.make_params, dtype, seed)
 # The first case is the reference's own comparison-test configuration
@@ -53,6 +57,20 @@ CASES = [
                              resampling_coeffs=(0.5, 1020.0, -20.0, 10.0), windowing=True, window_type=0,
                              window_center=0.5, window_fill=0.95, fpn_removal=True, fpn_bscan_count=1,
                              grayscale_min=20.0, grayscale_max=110.0), 16),
+    # the benchmark workload's shape: 2048 samples, cubic, Gaussian window,
+    # dispersion compensation, FPN determined from the frame, spectra from the
+    # benchmark generator with a fixed-pattern background ripple
+    ("headline_cubic_gauss_fpn_n2048", dict(n=2048, ascans=64, dtype=2, resampling=True, interpolation=1,
+                                            resampling_coeffs=_LIN2048, windowing=True, window_type=1,
+                                            window_center=0.5, window_fill=0.9, dispersion=True,
+                                            dispersion_coeffs=_DISP, fpn_removal=True, fpn_bscan_count=1,
+                                            grayscale_min=30.0, grayscale_max=110.0, gen="bench"), 17),
+    # rolling-average DC removal where the reference's float prefix sums round (N = 4096)
+    ("dc_lanczos_n4096", dict(n=4096, ascans=8, dtype=2, resampling=True, interpolation=2,
+                              resampling_coeffs=(0.5, 4090.0, -40.0, 20.0), windowing=True, window_type=0,
+                              window_center=0.5, window_fill=0.95, dispersion=True,
+                              dispersion_coeffs=(0.0, 0.0, 2.0, -1.0), dc_removal=True, dc_window=64,
+                              grayscale_min=20.0, grayscale_max=110.0), 18),
 ]
 
 
@@ -67,15 +85,23 @@ def raw_for(n, m, dtype, seed):
     return np.clip(v + 20000, 0, 65535).astype(np.uint16)
 
 
-def main():
+def main(names=()):
     if not reflib.available():
         reflib.build()
     reflib.set_fft_precision("f64")
     for name, kw, seed in CASES:
+        if names and name not in names:
+            continue
+        kw = dict(kw)
         n, m = kw.pop("n"), kw.pop("ascans")
         dtype = kw.pop("dtype")
+        gen = kw.pop("gen", None)
         p = reflib.make_params(n, m, 1, dtype, **kw)
-        raw = raw_for(n, m, dtype, seed)
+        if gen == "bench":
+            raw = synth.as_numpy(synth.generate(synth.SynthParams(n=n, ascans=m, seed=seed, d2=12.0, d3=-6.0,
+                                                                  background_ripple=True)), "uint16")
+        else:
+            raw = raw_for(n, m, dtype, seed)
         r, w, ph, cs = reflib.generate_curves(p)
         be = reflib.RefBackend(p)
         if kw.get("fpn_removal"):
@@ -99,4 +125,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -28,7 +28,7 @@ class EmuArgs(ctypes.Structure):
                 ("dc_window", ctypes.c_int), ("log_scaling", ctypes.c_int), ("gmin", ctypes.c_float),
                 ("gmax", ctypes.c_float), ("addend", ctypes.c_float), ("mult", ctypes.c_float),
                 ("flip", ctypes.c_int), ("ascans_per_bscan", ctypes.c_int), ("bscans", ctypes.c_int),
-                ("dc_split", ctypes.c_int)]
+                ("dc_split", ctypes.c_int), ("dc_ref_order", ctypes.c_int)]
 
 
 def emu_lib():
@@ -60,7 +60,7 @@ def emu_run(L, spec: ChainSpec, raw: np.ndarray, what: str = "image", fpn=None) 
                 _ptr(cs) if spec.dispersion else None, _ptr(fp),
                 spec.dc_window if spec.dc_removal else 0, int(spec.log_scaling), spec.grayscale_min,
                 spec.grayscale_max, spec.addend, spec.multiplicator, int(spec.bscan_flip),
-                spec.ascans_per_bscan, spec.bscans_per_buffer, int(spec.dc_split))
+                spec.ascans_per_bscan, spec.bscans_per_buffer, int(spec.dc_split), int(spec.dc_reference_order))
     code = {"image": 0, "fft_input": 1, "bins": 2, "resampled": 3}[what]
     if what == "resampled":
         out = np.zeros((m, n), np.float32)
@@ -96,6 +96,18 @@ def oracle_settings(spec: ChainSpec):
 def oracle_image(spec: ChainSpec, raw, mode="ref", **kw):
     st, cur = oracle_settings(spec)
     return R.process_buffer(raw, st, cur, mode=mode, **kw)
+
+
+def fpn_kappa(spec: ChainSpec, X64: np.ndarray, fpn) -> np.ndarray:
+    """Fixed-pattern cancellation factor kappa = |X| / |X - F| per kept bin (X the
+    float64 DFT bin, F the FPN profile as interleaved pairs); 1 without FPN."""
+    half = spec.signal_length // 2
+    if fpn is None:
+        return np.ones((X64.shape[0], half))
+    F = fpn[0::2].astype(np.float64) + 1j * fpn[1::2].astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        k = np.abs(X64[:, :half]) / np.abs(X64[:, :half] - F[None, :half])
+    return np.nan_to_num(np.maximum(k, 1.0), nan=1.0, posinf=1e30)
 
 
 def to_db(out: np.ndarray, spec: ChainSpec) -> np.ndarray:
