@@ -16,9 +16,19 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libope_cpu_ref.so")
-# Source tree of the reference (read-only), named by the environment; there is
-# no default. Without it the prebuilt _ref/ libraries are used as they are.
-REFERENCE_TREE = os.environ.get("OPE_REFERENCE_TREE", "")
+# Source tree of the reference (read-only), named by the environment or, failing
+# that, recorded by the last oracle build (_ref/reference_tree.txt); there is no
+# default. Without either the prebuilt _ref/ libraries are used as they are.
+def _reference_tree() -> str:
+    t = os.environ.get("OPE_REFERENCE_TREE", "")
+    rec = os.path.join(HERE, "_ref", "reference_tree.txt")
+    if not t and os.path.exists(rec):
+        with open(rec) as f:
+            t = f.read().strip()
+    return t if t and os.path.isdir(t) else ""
+
+
+REFERENCE_TREE = _reference_tree()
 
 
 class RefParams(ctypes.Structure):

@@ -242,7 +242,9 @@ def test_host_library_exports():
     ctypes.CDLL(B.HOST_LIB)
 
 
-REF_EXAMPLE = os.path.join(os.environ.get("OPE_REFERENCE_TREE", "/nonexistent"), "examples", "example_basic.cpp")
+from oracle.reflib import REFERENCE_TREE  # noqa: E402  (named by the environment or the oracle build)
+
+REF_EXAMPLE = os.path.join(REFERENCE_TREE or "/nonexistent", "examples", "example_basic.cpp")
 
 
 @pytest.mark.skipif(not os.path.exists(REF_EXAMPLE), reason="reference sources not present")
