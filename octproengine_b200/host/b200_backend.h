@@ -6,7 +6,15 @@
 
 #include <memory>
 
+// Built into the reference library (the Backend::B200 patch), the class derives
+// from the reference's own ProcessingBackend: that build names its
+// src/backends/backend_interface.h here. This library's own host layer uses the
+// interface declared beside this file.
+#if defined(OPE_B200_REFERENCE_INTERFACE)
+#include OPE_B200_REFERENCE_INTERFACE
+#else
 #include "backend_interface.h"
+#endif
 
 namespace ope {
 

@@ -39,15 +39,19 @@ public:
     }
 
     void createBackend(Backend type) {
+        // This library is the single-backend build: Backend::CPU and
+        // Backend::CUDA are the OCTproEngine library's own backends, which hold
+        // all three once B200Backend is added to it (the Backend::B200 patch).
         switch (type) {
             case Backend::B200:
-            case Backend::CUDA:  // the GPU backend of this library is the sm_100a one
                 backend = std::make_unique<B200Backend>();
                 break;
             case Backend::CPU:
-                throw std::runtime_error(
-                    "This library provides the GPU (B200) backend only; Backend::CPU belongs to the "
-                    "OCTproEngine library itself");
+            case Backend::CUDA:
+                throw std::invalid_argument(
+                    std::string("Backend::") + (type == Backend::CPU ? "CPU" : "CUDA") +
+                    " is not in this build, which holds the B200 backend only: select Backend::B200, or build "
+                    "the OCTproEngine library with the Backend::B200 patch to have all three side by side");
             default:
                 throw std::runtime_error("Unknown backend type");
         }

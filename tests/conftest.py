@@ -53,6 +53,19 @@ def refcuda():
 
 
 @pytest.fixture(scope="session")
+def dropin():
+    """The reference library built with the Backend::B200 patch (oracle/_ref)."""
+    from oracle import dropin as D
+    try:
+        D.build()
+    except Exception as e:  # pragma: no cover - depends on the machine
+        pytest.skip(f"drop-in reference library not buildable here: {e}")
+    if not D.available():
+        pytest.skip("drop-in reference library not present")
+    return D
+
+
+@pytest.fixture(scope="session")
 def cuda():
     import torch
     if not torch.cuda.is_available():

@@ -40,7 +40,7 @@ int main(int argc, char** argv) {
         }
     }
     try {
-        ope::Processor proc(ope::Backend::CUDA);
+        ope::Processor proc(ope::Backend::B200);
         proc.setInputParameters(n, a, b, ope::DataType::UINT16);
         const float res[4] = {0.5f, static_cast<float>(n - 1) - 40.0f, 60.0f, -20.0f};
         proc.setResamplingCoefficients(res);

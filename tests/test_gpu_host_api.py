@@ -168,7 +168,7 @@ def test_processor_stream_matches_c_abi(ope, cuda):
     spec = _spec()
     frames = _frames(spec, 6, seed=11)
     want = _reference_outputs(spec, frames)
-    with ope.Processor(ope.Backend.CUDA) as proc:
+    with ope.Processor(ope.Backend.B200) as proc:
         _configure(ope, proc, spec)
         proc.initialize()
         c1, c2 = _Collector(), _Collector()
@@ -204,7 +204,7 @@ def test_processor_hot_swap_takes_effect(ope, cuda):
     spec = _spec(n=1024, a=256, b=2)
     frames = _frames(spec, 3, seed=21)
     col = _Collector()
-    with ope.Processor(ope.Backend.CUDA) as proc:
+    with ope.Processor(ope.Backend.B200) as proc:
         _configure(ope, proc, spec)
         proc.set_callback(col)
         proc.initialize()
@@ -231,7 +231,7 @@ def test_processor_fpn_determination_and_files(ope, cuda, tmp_path):
     spec = _spec(n=1024, a=256, b=2, fpn_removal=True, fpn_bscan_count=1)
     frames = _frames(spec, 2, seed=31)
     col = _Collector()
-    with ope.Processor(ope.Backend.CUDA) as proc:
+    with ope.Processor(ope.Backend.B200) as proc:
         _configure(ope, proc, spec)
         proc.enable_fixed_pattern_noise_removal(True)
         proc.set_fixed_pattern_noise_bscan_count(1)
@@ -264,7 +264,7 @@ def test_processor_reinitializes_on_new_dimensions(ope, cuda):
     spec_b = _spec(n=2048, a=64, b=2)
     fa, fb = _frames(spec_a, 1, seed=50)[0], _frames(spec_b, 1, seed=51)[0]
     col = _Collector()
-    with ope.Processor(ope.Backend.CUDA) as proc:
+    with ope.Processor(ope.Backend.B200) as proc:
         _configure(ope, proc, spec_a)
         proc.set_callback(col)
         proc.initialize()

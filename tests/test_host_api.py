@@ -150,8 +150,8 @@ def test_ini_roundtrip(ope, tmp_path):
 
 
 def test_processor_without_device(ope, tmp_path):
-    p = ope.Processor(ope.Backend.CUDA)
-    assert p.get_backend() == ope.Backend.CUDA and "CUDA" in repr(p)
+    p = ope.Processor(ope.Backend.B200)
+    assert p.get_backend() == ope.Backend.B200 and "B200" in repr(p)
     p.set_input_parameters(1024, 256, 1, ope.DataType.UINT16)
     cfg = p.config
     assert cfg.data.signal_length == 1024 and cfg.data.samples_per_buffer == 1024 * 256
@@ -190,7 +190,7 @@ def test_processor_without_device(ope, tmp_path):
     with open(path) as f:
         lines = f.read().splitlines()
     assert lines[0] == "Sample Number;Sample Value" and lines[1] == "0;0" and len(lines) == 513
-    q = ope.Processor(ope.Backend.CUDA)
+    q = ope.Processor(ope.Backend.B200)
     q.set_input_parameters(1024, 256, 1, ope.DataType.UINT16)
     q.load_post_process_background_profile_from_file(path)
     np.testing.assert_allclose(q.get_post_process_background_profile(), bg, rtol=1e-5)
@@ -209,19 +209,26 @@ def test_processor_without_device(ope, tmp_path):
         q.load_config(str(tmp_path / "nope.ini"))
 
 
-def test_cpu_backend_not_provided(ope):
-    with pytest.raises(RuntimeError, match="CPU"):
-        ope.Processor(ope.Backend.CPU)
+def test_single_backend_build_selects_b200_only(ope):
+    """libope_host.so holds the B200 backend alone: Backend::CPU and
+    Backend::CUDA (the reference library's own backends) are refused with an
+    argument error naming the backend, never silently replaced; the reference
+    library built with the Backend::B200 patch holds all three
+    (tests/test_dropin.py)."""
+    for b, name in ((ope.Backend.CPU, "CPU"), (ope.Backend.CUDA, "CUDA")):
+        with pytest.raises(ValueError, match=name):
+            ope.Processor(b)
     p = ope.Processor(ope.Backend.B200)
-    with pytest.raises(RuntimeError):
+    with pytest.raises(ValueError):
         p.set_backend(ope.Backend.CPU)
+    assert p.get_backend() == ope.Backend.B200
 
 
 def test_initialize_without_device_raises(ope):
     import torch
     if torch.cuda.is_available():
         pytest.skip("a device is present")
-    p = ope.Processor(ope.Backend.CUDA)
+    p = ope.Processor(ope.Backend.B200)
     p.set_input_parameters(1024, 64, 1, ope.DataType.UINT16)
     with pytest.raises(ope.InitializationError):
         p.initialize()
@@ -250,7 +257,8 @@ REF_EXAMPLE = os.path.join(REFERENCE_TREE or "/nonexistent", "examples", "exampl
 @pytest.mark.skipif(not os.path.exists(REF_EXAMPLE), reason="reference sources not present")
 def test_reference_example_builds_against_headers(tmp_path):
     """The reference's example program compiles and links, unmodified, against
-    include/ope and libope_host.so (it selects Backend::CUDA)."""
+    include/ope and libope_host.so (it selects Backend::CUDA, which this
+    single-backend build refuses at run time; the build and link are checked)."""
     B.build()
     exe = str(tmp_path / "example_basic")
     cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include", "ope"), REF_EXAMPLE, "-o", exe,
