@@ -357,7 +357,8 @@ OPE_HD void phase_split_store(int t, const float2* vals, float2 c, float2* spec)
 // bytes of the float pair. A tap is converted in registers exactly:
 // (2^23 + u) - (2^23 + c) = u - c, the same float as the float spectrum holds.
 
-OPE_HD float2 packed_to_pair(uint32_t w, float2 cbias) {
+// The pair (2^23 + u_a, 2^23 + u_b) of a packed word: exact floats, no arithmetic.
+OPE_HD float2 packed_biased(uint32_t w) {
 #if defined(__CUDA_ARCH__)
     const float lo = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5410));
     const float hi = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5432));
@@ -365,8 +366,10 @@ OPE_HD float2 packed_to_pair(uint32_t w, float2 cbias) {
     const float lo = bits_f(static_cast<int>(0x4B000000u | (w & 0xFFFFu)));
     const float hi = bits_f(static_cast<int>(0x4B000000u | (w >> 16)));
 #endif
-    return sub2(make_float2(lo, hi), cbias);
+    return make_float2(lo, hi);
 }
+
+OPE_HD float2 packed_to_pair(uint32_t w, float2 cbias) { return sub2(packed_biased(w), cbias); }
 
 // Samples 2p and 2p+1 of both rows as packed words; adds them to the row sums.
 template <int DT>
@@ -728,9 +731,10 @@ OPE_HD void phase_prestage_packed(int t, const uint32_t* specw, float2 cbias, co
             const int2 e = a.lin[j];
 #endif
             OPE_SMEM_CHECK(e.x >= 0 && e.x + 1 < N + 2 * SPEC_PAD);
-            const float2 y1 = packed_to_pair(specw[e.x], cbias);
-            const float2 y2 = packed_to_pair(specw[e.x + 1], cbias);
-            y = add2(y1, mul2x(sub2(y2, y1), dup2(bits_f(e.y)), NZ));
+            // y2 - y1 is the exact difference of the biased taps
+            const float2 Y1 = packed_biased(specw[e.x]);
+            const float2 d = sub2(packed_biased(specw[e.x + 1]), Y1);
+            y = add2(sub2(Y1, cbias), mul2x(d, dup2(bits_f(e.y)), NZ));
         } else if (INTERP == INTERP_CUBIC) {
 #if defined(__CUDA_ARCH__)
             const int2 e = __ldg(a.cub + j);
@@ -740,15 +744,20 @@ OPE_HD void phase_prestage_packed(int t, const uint32_t* specw, float2 cbias, co
             const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
             OPE_SMEM_CHECK(i0 < N + 2 * SPEC_PAD && i1 + 2 < N + 2 * SPEC_PAD);
             const float pos = bits_f(e.y), pos2 = fmul_rn(pos, pos);
-            const float2 y0 = packed_to_pair(specw[i0], cbias), y1 = packed_to_pair(specw[i1], cbias);
-            const float2 y2 = packed_to_pair(specw[i1 + 1], cbias), y3 = packed_to_pair(specw[i1 + 2], cbias);
-            float2 ca = add2(sub2(mul2x(dup2(3.0f), sub2(y1, y2), NZ), y0), y3);
-            float2 cb = sub2(add2(sub2(mul2x(dup2(2.0f), y0, NZ), mul2x(dup2(5.0f), y1, NZ)),
-                                  mul2x(dup2(4.0f), y2, NZ)),
-                             y3);
-            float2 cc = sub2(y2, y0);
-            float2 in = add2(add2(mul2x(ca, dup2(pos2), NZ), mul2x(cb, dup2(pos), NZ)), cc);
-            y = add2(mul2x(dup2(fmul_rn(0.5f, pos)), in, NZ), y1);
+            // cubicHermiteInterpolation (cpu_kernels.tpp:486-502) on integer taps
+            // y_k = u_k - c: its a, b, c are integers below 2^20, exact in any
+            // evaluation order, so they are formed from differences of the
+            // biased taps Y_k = 2^23 + u_k (exact, no conversion); with
+            // na = -a, fl(a pos^2) = -fl(na pos^2), so the reference's
+            // ((a pos^2 + b pos) + c) is (b pos - na pos^2) + c, bit for bit.
+            const float2 Y0 = packed_biased(specw[i0]), Y1 = packed_biased(specw[i1]);
+            const float2 Y2 = packed_biased(specw[i1 + 1]), Y3 = packed_biased(specw[i1 + 2]);
+            const float2 e0 = sub2(Y0, Y1), e2 = sub2(Y2, Y1), e3 = sub2(Y1, Y3);
+            const float2 na = fma2(dup2(3.0f), e2, add2(e0, e3));      // y0 - 3(y1 - y2) - y3
+            const float2 cb = fma2(dup2(2.0f), e0, fma2(dup2(4.0f), e2, e3));  // 2y0 - 5y1 + 4y2 - y3
+            const float2 cc = sub2(e2, e0);                            // y2 - y0
+            const float2 in = add2(sub2(mul2x(cb, dup2(pos), NZ), mul2x(na, dup2(pos2), NZ)), cc);
+            y = add2(mul2x(dup2(fmul_rn(0.5f, pos)), in, NZ), sub2(Y1, cbias));
         } else {
             const int b = a.lz_base[j];
             OPE_SMEM_CHECK(b >= 0 && b + 15 < N + 2 * SPEC_PAD);
@@ -764,6 +773,12 @@ OPE_HD void phase_prestage_packed(int t, const uint32_t* specw, float2 cbias, co
             }
             y = acc;
         }
+#if !defined(__CUDA_ARCH__)
+        if (a.resampled_out) {  // CPU emulation only: the k-linearised spectrum of this pair
+            a.resampled_out[(long long)j * 2] = y.x;
+            a.resampled_out[(long long)j * 2 + 1] = y.y;
+        }
+#endif
 #if defined(__CUDA_ARCH__)
         const float2 q = __ldg(a.wph + j);
 #else

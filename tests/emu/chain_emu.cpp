@@ -89,12 +89,34 @@ int emu_run(const EmuArgs& e, int what, float* out) {
     const size_t row_bytes = N * sizeof(raw_t);
     const unsigned char* in = static_cast<const unsigned char*>(e.in);
 
+    // 8/16-bit samples without rolling-average DC removal: the kernel keeps the
+    // spectrum as packed integer words (phase_store_packed) and interpolates
+    // from them (phase_prestage_packed); the emulation runs the same phases
+    constexpr bool PACKABLE = (DT == IN_U8 || DT == IN_U16);
+    const bool packed = PACKABLE && e.dc_window == 0;
+    float2 cbias = make_float2(8388608.0f, 8388608.0f);
+
     for (long long r = 0; r < e.m; r += 2) {
         const bool has_b = r + 1 < e.m;
         std::memcpy(stage.data(), in + r * row_bytes, row_bytes * (has_b ? 2 : 1));
         if (!has_b) std::memset(stage.data() + row_bytes, 0, row_bytes);
         float2 dc = make_float2(0.0f, 0.0f);
-        if (e.dc_window == 0 && a.dc_resp) {
+        cbias = make_float2(8388608.0f, 8388608.0f);
+        if (packed) {
+            std::vector<std::array<uint32_t, 16>> words(T);
+            long long ta = 0, tb = 0;  // exact integer sums: any order
+            for (int t = 0; t < T; ++t) {
+                int sa = 0, sb = 0;
+                phase_split_load_packed<N, DT>(t, stage.data(), words[t].data(), &sa, &sb);
+                ta += sa;
+                tb += sb;
+            }
+            if (a.dc_resp) {
+                dc = make_float2(split_level((double)ta, N, true), split_level((double)tb, N, true));
+                cbias = add2(cbias, dc);
+            }
+            for (int t = 0; t < T; ++t) phase_store_packed<N>(t, words[t].data(), reinterpret_cast<uint32_t*>(spec));
+        } else if (e.dc_window == 0 && a.dc_resp) {
             // same reduction tree as team_sum2: xor butterfly per warp, lane 0, then warps in order
             using SS = typename SplitSum<DT>::type;
             std::vector<std::array<float2, 16>> vals(T);
@@ -167,7 +189,12 @@ int emu_run(const EmuArgs& e, int what, float* out) {
             rs.assign(2 * N, 0.0f);
             a.resampled_out = rs.data();
         }
-        for (int t = 0; t < T; ++t) phase_prestage<N, INTERP>(t, spec, a, v[t].data());
+        for (int t = 0; t < T; ++t) {
+            if (packed)
+                phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v[t].data());
+            else
+                phase_prestage<N, INTERP>(t, spec, a, v[t].data());
+        }
         a.resampled_out = nullptr;
         if (what == OUT_RESAMPLED) {
             for (int j = 0; j < N; ++j) {
