@@ -21,6 +21,9 @@ becomes a gradient fit.
   normalised intensity, differentiable with respect to ``params``;
 * :func:`fit_dispersion` -- BFGS on (d2, d3) of the centred dispersion phase
   psi(t) = d2 (t-1/2)^2 + d3 (t-1/2)^3, entropy objective;
+* :func:`fit_dispersion_kmap` -- BFGS on (d2, d3) and the parameters of a
+  k-map family (the resampling coefficients as a function of a few physical
+  parameters), with the full adjoint's k-map gradient;
 * :func:`grid_sweep` -- the parameter sweep it replaces, every grid point one
   launch of the same forward chain, all enqueued back to back.
 
@@ -294,6 +297,65 @@ class FitEvaluator:
         return float(self.h_hs[0]), g
 
 
+class KmapFitEvaluator(FitEvaluator):
+    """H and its gradient with respect to (d2, d3, kappa_1 .. kappa_K), where the
+    resampling coefficients are ``kmap_of(kappa)`` -> (c0..c3), a k-map family
+    given by the caller (for example the inverse of a physical wavenumber map
+    with a few free coefficients). Per evaluation: forward and the FULL adjoint
+    (dH/dc0..c3 as well as dH/dd0..d3), replayed from one CUDA graph; the chain
+    rule through ``kmap_of`` runs on the host with a central-difference
+    Jacobian (``dkappa``)."""
+
+    def __init__(self, af: Autofocus, raw: torch.Tensor, kmap_of, k0: Sequence[float], dkappa: float = 1e-4,
+                 graph: bool = True):
+        self.kmap_of = kmap_of
+        self.dkappa = float(dkappa)
+        self.nk = len(k0)
+        super().__init__(af, raw, kmap_of(np.asarray(k0, np.float64)), graph=graph)
+
+    def _set(self, theta) -> None:
+        theta = np.asarray(theta, np.float64)
+        hp = self.h_params.numpy()
+        hp[:4] = dispersion_poly(theta[0], theta[1])
+        if theta.size > 2:
+            hp[4:] = np.asarray(self.kmap_of(theta[2:]), np.float32)
+        else:
+            hp[4:] = self.kmap
+
+    def _enqueue(self, stream) -> None:
+        self._copy(self.d_params, self.h_params, stream)
+        self.af.forward(self.raw, self.d_params, hs=self.d_hs, stream=stream)
+        grad = self.h_grad if self.sm_copies else self.d_grad
+        self.af.backward(self.raw, self.d_params, grad, hs=self.d_hs, stream=stream, dispersion_only=False)
+        self._copy(self.h_hs, self.d_hs, stream)
+        if not self.sm_copies:
+            self._copy(self.h_grad, self.d_grad, stream)
+
+    def jacobian(self, kappa: np.ndarray) -> np.ndarray:
+        """d(c0..c3)/d(kappa), 4 x K, central differences."""
+        J = np.empty((4, self.nk))
+        for i in range(self.nk):
+            e = np.zeros(self.nk)
+            e[i] = self.dkappa
+            J[:, i] = (np.asarray(self.kmap_of(kappa + e), np.float64) -
+                       np.asarray(self.kmap_of(kappa - e), np.float64)) / (2 * self.dkappa)
+        return J
+
+    def __call__(self, theta: np.ndarray):
+        theta = np.asarray(theta, np.float64)
+        self._set(theta)
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._enqueue(self.stream)
+        torch.cuda.current_stream(self.raw.device).synchronize()
+        self.count += 1
+        g8 = self.h_grad.numpy().astype(np.float64)
+        gd = CENTRED_TO_POLY.T @ g8[:4]
+        gk = self.jacobian(theta[2:]).T @ g8[4:]
+        return float(self.h_hs[0]), np.concatenate([gd, gk])
+
+
 def _allreduce_sum(values: np.ndarray, group=None) -> np.ndarray:
     """Sum over the ranks of `group` in float64 (on the device under NCCL, on the host under gloo)."""
     import torch.distributed as dist
@@ -429,6 +491,86 @@ def fit_dispersion(af: Autofocus, raw: torch.Tensor, kmap: Sequence[float], init
             break
     secs = time.perf_counter() - t0
     return FitResult(float(x[0]), float(x[1]), f, it, ev.count - count0, secs, hist)
+
+
+@dataclass
+class JointFitResult:
+    d2: float
+    d3: float
+    kappa: np.ndarray  # the fitted k-map family parameters
+    kmap: np.ndarray  # the resampling coefficients c0..c3 they give
+    entropy: float
+    iterations: int
+    evaluations: int
+    seconds: float
+    history: list = field(default_factory=list)  # (theta, H, seconds since start) per iteration
+
+
+def _bfgs(ev, x0: np.ndarray, scale: np.ndarray, max_iter: int, step_tol: float, first_step: float):
+    """BFGS with Armijo backtracking in the scaled coordinates y = x / scale."""
+    t0 = time.perf_counter()
+    n = x0.size
+
+    def fy(y):
+        f, g = ev(y * scale)
+        return f, g * scale
+
+    y = x0 / scale
+    f, g = fy(y)
+    gmax = float(np.abs(g).max())
+    hinv = np.eye(n) * (first_step / gmax if gmax > 0 else 1.0)
+    hist = [(y * scale, f, time.perf_counter() - t0)]
+    it = 0
+    for it in range(1, max_iter + 1):
+        d = -hinv @ g
+        if g @ d >= 0:
+            hinv = np.eye(n) * (first_step / max(float(np.abs(g).max()), 1e-30))
+            d = -hinv @ g
+        step = 1.0
+        while True:
+            yn = y + step * d
+            fn, gn = fy(yn)
+            if fn <= f + 1e-4 * step * float(g @ d) or step < 1e-6:
+                break
+            step *= 0.5
+        s, yv = yn - y, gn - g
+        sy = float(s @ yv)
+        if sy > 1e-30:
+            rho = 1.0 / sy
+            eye = np.eye(n)
+            hinv = (eye - rho * np.outer(s, yv)) @ hinv @ (eye - rho * np.outer(yv, s)) + rho * np.outer(s, s)
+        y, f, g = yn, fn, gn
+        hist.append((y * scale, f, time.perf_counter() - t0))
+        if float(np.linalg.norm(s)) < step_tol:  # a step below step_tol in the scaled coordinates
+            break
+    return y * scale, f, it, time.perf_counter() - t0, hist
+
+
+def fit_dispersion_kmap(af: Autofocus, raw: torch.Tensor, kmap_of, k0: Sequence[float], init=(0.0, 0.0),
+                        kappa_scale: Optional[Sequence[float]] = None, max_iter: int = 120, step_tol: float = 1e-3,
+                        first_step: float = 2.0, graph: bool = True, evaluator=None) -> JointFitResult:
+    """Minimises the image entropy jointly over the centred dispersion (d2, d3)
+    and the parameters kappa of a k-map family: the resampling coefficients
+    are ``kmap_of(kappa)``, starting from ``k0`` (the nominal k-map).
+
+    A fit over the four raw resampling coefficients is ill-posed: on scenes of
+    a few reflectors the entropy cannot tell a cubic k-map error from cubic
+    dispersion. A k-map family with the physics' own few free parameters (for
+    instance the cubic coefficient of the wavenumber map) is not: a k-map
+    error shifts the phase of each reflector in proportion to its depth,
+    dispersion does not, so the joint optimum separates them.
+    ``kappa_scale``: typical size of one unit of each kappa relative to a
+    radian of (d2, d3) for the optimiser's coordinates (default 0.01).
+    """
+    k0 = np.asarray(k0, np.float64)
+    ev = evaluator if evaluator is not None else KmapFitEvaluator(af, raw, kmap_of, k0, graph=graph)
+    count0 = ev.count
+    x0 = np.concatenate([np.asarray(init, np.float64), k0])
+    ks = np.full(k0.size, 0.01) if kappa_scale is None else np.asarray(kappa_scale, np.float64)
+    scale = np.concatenate([[1.0, 1.0], ks])
+    x, f, it, secs, hist = _bfgs(ev, x0, scale, max_iter, step_tol, first_step)
+    return JointFitResult(float(x[0]), float(x[1]), x[2:].copy(), np.asarray(kmap_of(x[2:]), np.float64), f, it,
+                          ev.count - count0, secs, hist)
 
 
 @dataclass

@@ -84,6 +84,31 @@ def linearising_coeffs(n: int, coeffs=K_COEFFS) -> tuple:
     return tuple(float(v) for v in sol)
 
 
+class KmapFamily:
+    """The resampling coefficients c0..c3 that linearise the wavenumber map
+    k(n) = K0 + K1 n + K2 n^2 + K3 s n^3, as a function of the scale s of its
+    cubic coefficient (the perturbation of the autofocus workload): one free
+    physical parameter instead of four raw coefficients. Tabulated once on a
+    fine grid of s and interpolated with cubic splines, so an evaluation costs
+    microseconds on the host."""
+
+    def __init__(self, n: int, coeffs=K_COEFFS, s_range=(0.5, 1.5), points: int = 401):
+        from scipy.interpolate import CubicSpline
+        self.n = n
+        self.coeffs = tuple(coeffs)
+        self.s = np.linspace(s_range[0], s_range[1], points)
+        tab = np.array([linearising_coeffs(n, self.k_coeffs(s)) for s in self.s])
+        self._spline = CubicSpline(self.s, tab, axis=0)
+
+    def k_coeffs(self, s: float) -> tuple:
+        c = list(self.coeffs)
+        c[3] = c[3] * float(s)
+        return tuple(c)
+
+    def __call__(self, kappa) -> np.ndarray:
+        return self._spline(float(np.asarray(kappa).reshape(-1)[0]))
+
+
 def compensating_coeffs(d2: float, d3: float) -> tuple:
     """Dispersion coefficients (d0..d3 over t) whose phase equals psi(t).
 

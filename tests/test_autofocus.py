@@ -188,6 +188,77 @@ def test_fit_recovers_hidden_dispersion(cuda):
     assert err < 0.01, (res, d2, d3)
 
 
+def test_kmap_family_interpolates_the_linearising_coefficients():
+    fam = synth.KmapFamily(N)
+    for sc in (0.81, 1.0, 1.137):
+        want = np.array(synth.linearising_coeffs(N, fam.k_coeffs(sc)))
+        assert np.allclose(fam(sc), want, rtol=0, atol=1e-6 * np.abs(want).max())
+
+
+def test_kmap_is_identifiable_by_entropy_in_float64():
+    """The objective, not the arithmetic: in float64, BFGS on (d2, d3, s) from
+    d = 0 and the nominal k-map (s = 1) ends at the hidden (d2, d3, s) of a
+    five-reflector scene -- a k-map error moves each reflector's phase in
+    proportion to its depth, dispersion does not."""
+    from scipy.optimize import minimize
+    from octproengine_b200.autofocus import dispersion_poly, CENTRED_TO_POLY
+    fam = synth.KmapFamily(N)
+    d2, d3, st = -19.07, -8.06, 1.1257
+    ctrue = synth.linearising_coeffs(N, fam.k_coeffs(st))
+    raw = synth.as_numpy(synth.generate(synth.SynthParams(n=N, ascans=64, seed=72, d2=d2, d3=d3,
+                                                          resampling_truth=ctrue)), "uint16")
+    window = R.window_curve(N, R.HANN, 0.5, 0.95)
+
+    def fg(y):  # y = (d2, d3, 100 (s - 1))
+        s = 1.0 + 0.01 * y[2]
+        J = (fam(s + 1e-4) - fam(s - 1e-4)) / 2e-4
+        H, g = O.entropy_and_grad(raw, np.concatenate([dispersion_poly(y[0], y[1]), fam(s)]), window, O.LANCZOS,
+                                  f32_curves=False)
+        return H, np.concatenate([CENTRED_TO_POLY.T @ g[:4], [0.01 * float(g[4:] @ J)]])
+
+    r = minimize(fg, np.zeros(3), jac=True, method="BFGS", options={"gtol": 1e-9, "maxiter": 200})
+    s = 1.0 + 0.01 * r.x[2]
+    assert abs(s - st) / st < 0.005 and abs(r.x[0] - d2) / abs(d2) < 0.02 and abs(r.x[1] - d3) / abs(d3) < 0.02, r.x
+
+
+@pytest.mark.gpu
+def test_kmap_fit_gradient_matches_fp64(cuda):
+    """dH/d(d2, d3, s) of KmapFitEvaluator (full adjoint on the GPU, chain rule
+    through the k-map family on the host) against float64 autograd."""
+    from octproengine_b200.autofocus import KmapFitEvaluator, dispersion_poly, CENTRED_TO_POLY
+    fam = synth.KmapFamily(N)
+    raw_t, raw, window, _ = make_case(m=128, seed=31, d2=14.0, d3=-6.0, kpert=0.9)
+    af = _af(cuda, O.LANCZOS, window)
+    ev = KmapFitEvaluator(af, raw_t.to(cuda), fam, [1.0])
+    theta = np.array([10.0, -4.0, 0.95])
+    H, g = ev(theta)
+    p64 = np.concatenate([dispersion_poly(theta[0], theta[1]), fam(theta[2])])
+    H64, g64 = O.entropy_and_grad(raw, p64, window, O.LANCZOS)
+    J = (fam(theta[2] + 1e-4) - fam(theta[2] - 1e-4)) / 2e-4
+    want = np.concatenate([CENTRED_TO_POLY.T @ g64[:4], [float(g64[4:] @ J)]])
+    assert abs(H - H64) <= 1e-5 * abs(H64)
+    assert np.all(np.abs(g - want) <= 0.01 * np.abs(want) + 1e-4 * np.abs(want).max()), (g, want)
+
+
+@pytest.mark.gpu
+def test_joint_fit_recovers_dispersion_and_kmap_from_the_nominal_kmap(cuda):
+    """fit_dispersion_kmap from d = 0 and the nominal k-map recovers the hidden
+    dispersion and the k-map's cubic coefficient (perturbed by 12.6 %) to 1 %."""
+    from octproengine_b200.autofocus import fit_dispersion_kmap
+    fam = synth.KmapFamily(N)
+    d2, d3, st = -19.07, -8.06, 1.1257
+    ctrue = synth.linearising_coeffs(N, fam.k_coeffs(st))
+    p = synth.SynthParams(n=N, ascans=512, seed=72, d2=d2, d3=d3, resampling_truth=ctrue)
+    raw_t = synth.generate(p)
+    window = R.window_curve(N, R.HANN, 0.5, 0.95)
+    af = _af(cuda, O.LANCZOS, window)
+    res = fit_dispersion_kmap(af, raw_t.to(cuda), fam, [1.0])
+    s = float(res.kappa[0])
+    errs = (abs(res.d2 - d2) / abs(d2), abs(res.d3 - d3) / abs(d3), abs(s - st) / st)
+    assert max(errs) < 0.01, (res, errs)
+    assert np.allclose(res.kmap, fam(s))
+
+
 @pytest.mark.gpu
 def test_reused_evaluator_serves_new_data_like_a_fresh_one(cuda):
     from octproengine_b200.autofocus import FitEvaluator, fit_dispersion
