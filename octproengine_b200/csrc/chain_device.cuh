@@ -322,10 +322,7 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
                 dc = make_float2(split_level((double)sa, N, true), split_level((double)sb, N, true));
                 cbias = add2(cbias, dc);  // 2^23 + c, exact for c < 2^23
             }
-            if constexpr (INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC)
-                phase_store_quad<N, DT>(t, stage, words, reinterpret_cast<float4*>(spec));
-            else
-                phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
+            phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
         } else if (a.dc_window > 0 && a.dc_ref_order) {
             phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
             tm.sync();
@@ -356,10 +353,7 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
 
         // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];
-        if constexpr (PACKABLE && (INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC)) {
-            if (packed) phase_prestage_quad<N, INTERP>(t, reinterpret_cast<const float4*>(spec), cbias, a, v);
-            else phase_prestage<N, INTERP>(t, spec, a, v);
-        } else if (packed) phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v);
+        if (packed) phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v);
         else phase_prestage<N, INTERP>(t, spec, a, v);
         fft_twiddle_dft<N, 0, false, S>(t, v, a.tw);
         tm.sync();  // spec aliases the exchange buffer

@@ -432,115 +432,6 @@ OPE_HD void phase_store_packed(int t, const uint32_t* words, uint32_t* specw) {
     }
 }
 
-// ---------------------------------------------- biased tap pairs (8/16-bit) --
-// For the 2- and 4-tap interpolations (linear, cubic) the packed words are
-// widened once, at the unpack, into entries of two neighbouring positions:
-// entry e = PAD + i holds (Y_a[i], Y_b[i], Y_a[i+1], Y_b[i+1]) with
-// Y = 2^23 + u the exact biased float of a sample (a byte permute, no
-// arithmetic), replicated edges. One 16-byte shared load then serves two taps
-// of both A-scans, and no tap needs converting in the gather: the
-// interpolation works on exact differences of biased taps.
-constexpr int QUAD_ENTRIES_PAD = SPEC_PAD;
-
-template <int N>
-struct QuadLayout {
-    static constexpr int ENTRIES = N + 2 * QUAD_ENTRIES_PAD;
-    static constexpr int BYTES = ENTRIES * 16;
-    static_assert(BYTES <= Plan<N>::EXCH_ELEMS * 16, "the tap-pair entries must fit the exchange region");
-};
-
-// Packed word of position i of both rows (row a low half, row b high half).
-template <int DT>
-OPE_HD uint32_t load_word_at(const unsigned char* stage, int n, int i) {
-    using raw_t = typename InTraits<DT>::raw_t;
-    const raw_t* ra = reinterpret_cast<const raw_t*>(stage);
-    return (uint32_t)ra[i] | ((uint32_t)ra[n + i] << 16);
-}
-
-OPE_HD float4 quad_of(float2 lo, float2 hi) { return make_float4(lo.x, lo.y, hi.x, hi.y); }
-
-// Step C of the tap-pair path: thread t writes entries PAD + 2p and PAD + 2p + 1
-// for its pairs p = t + k*T from its packed words (positions 2p, 2p+1) and the
-// word of position 2p+2 (re-read from the stage; position N replicates N-1).
-template <int N, int DT>
-OPE_HD void phase_store_quad(int t, const unsigned char* stage, const uint32_t* words, float4* Q) {
-    constexpr int T = Plan<N>::T;
-    constexpr int P = QUAD_ENTRIES_PAD;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int p = t + k * T;
-        const float2 y0 = packed_biased(words[2 * k]), y1 = packed_biased(words[2 * k + 1]);
-        const float2 y2 = (2 * p + 2 < N) ? packed_biased(load_word_at<DT>(stage, N, 2 * p + 2)) : y1;
-        OPE_SMEM_CHECK(P + 2 * p + 1 < QuadLayout<N>::ENTRIES);
-        Q[P + 2 * p] = quad_of(y0, y1);
-        Q[P + 2 * p + 1] = quad_of(y1, y2);
-        if (p == 0)
-            for (int e = 0; e < P; ++e) Q[e] = quad_of(y0, y0);
-        if (p == N / 2 - 1)
-            for (int e = 0; e < P; ++e) Q[P + N + e] = quad_of(y1, y1);
-    }
-}
-
-// Linear and cubic k-linearisation from the tap-pair entries; then the window
-// and phase factors, as phase_prestage.
-template <int N, int INTERP>
-OPE_HD void phase_prestage_quad(int t, const float4* Q, float2 cbias, const ChainArgs& a, cp* v) {
-    static_assert(INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC, "tap pairs serve the 2- and 4-tap kernels");
-    constexpr int T = Plan<N>::T;
-    const float2 NZ = dup2(a.neg_zero);
-    const float2* Qh = reinterpret_cast<const float2*>(Q);  // half entries: (Y_a[i], Y_b[i]) at 2*(PAD + i)
-#pragma unroll
-    for (int s = 0; s < 16; ++s) {
-        const int j = t + s * T;
-        float2 y;
-        if (INTERP == INTERP_LINEAR) {
-#if defined(__CUDA_ARCH__)
-            const int2 e = __ldg(a.lin + j);
-#else
-            const int2 e = a.lin[j];
-#endif
-            OPE_SMEM_CHECK(e.x >= 0 && e.x < QuadLayout<N>::ENTRIES);
-            // kLinearizationLinear (cpu_kernels.tpp:95-110): y1 + (y2 - y1) * (nx - n1)
-            const float4 q = Q[e.x];
-            const float2 Y1 = make_float2(q.x, q.y), Y2 = make_float2(q.z, q.w);
-            y = add2(sub2(Y1, cbias), mul2x(sub2(Y2, Y1), dup2(bits_f(e.y)), NZ));
-        } else {
-#if defined(__CUDA_ARCH__)
-            const int2 e = __ldg(a.cub + j);
-#else
-            const int2 e = a.cub[j];
-#endif
-            const int i0 = e.x & 0xFFFF, i1 = (unsigned)e.x >> 16;
-            OPE_SMEM_CHECK(i0 < QuadLayout<N>::ENTRIES && i1 + 2 < QuadLayout<N>::ENTRIES);
-            const float pos = bits_f(e.y), pos2 = fmul_rn(pos, pos);
-            // the same exact-difference form of cubicHermiteInterpolation as
-            // phase_prestage_packed
-            const float2 Y0 = Qh[2 * i0];
-            const float4 q = Q[i1];
-            const float2 Y1 = make_float2(q.x, q.y), Y2 = make_float2(q.z, q.w);
-            const float2 Y3 = Qh[2 * (i1 + 2)];
-            const float2 e0 = sub2(Y0, Y1), e2 = sub2(Y2, Y1), e3 = sub2(Y1, Y3);
-            const float2 na = fma2(dup2(3.0f), e2, add2(e0, e3));
-            const float2 cb = fma2(dup2(2.0f), e0, fma2(dup2(4.0f), e2, e3));
-            const float2 cc = sub2(e2, e0);
-            const float2 in = add2(sub2(mul2x(cb, dup2(pos), NZ), mul2x(na, dup2(pos2), NZ)), cc);
-            y = add2(mul2x(dup2(fmul_rn(0.5f, pos)), in, NZ), sub2(Y1, cbias));
-        }
-#if !defined(__CUDA_ARCH__)
-        if (a.resampled_out) {  // CPU emulation only: the k-linearised spectrum of this pair
-            a.resampled_out[(long long)j * 2] = y.x;
-            a.resampled_out[(long long)j * 2 + 1] = y.y;
-        }
-#endif
-#if defined(__CUDA_ARCH__)
-        const float2 wq = __ldg(a.wph + j);
-#else
-        const float2 wq = a.wph[j];
-#endif
-        v[s] = cpmake(mul2x(y, dup2(wq.x), NZ), mul2x(y, dup2(wq.y), NZ));
-    }
-}
-
 // DataParameters::bitshift as the reference's GPU path applies it
 // (inputToCufftComplex_and_bitshift, cuda_kernels.cu:45-63; the reference CPU
 // backend ignores the flag): every 8- or 16-bit sample shifted right by 4,

@@ -115,12 +115,7 @@ int emu_run(const EmuArgs& e, int what, float* out) {
                 dc = make_float2(split_level((double)ta, N, true), split_level((double)tb, N, true));
                 cbias = add2(cbias, dc);
             }
-            for (int t = 0; t < T; ++t) {
-                if constexpr (INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC)
-                    phase_store_quad<N, DT>(t, stage.data(), words[t].data(), reinterpret_cast<float4*>(spec));
-                else
-                    phase_store_packed<N>(t, words[t].data(), reinterpret_cast<uint32_t*>(spec));
-            }
+            for (int t = 0; t < T; ++t) phase_store_packed<N>(t, words[t].data(), reinterpret_cast<uint32_t*>(spec));
         } else if (e.dc_window == 0 && a.dc_resp) {
             // same reduction tree as team_sum2: xor butterfly per warp, lane 0, then warps in order
             using SS = typename SplitSum<DT>::type;
@@ -195,10 +190,7 @@ int emu_run(const EmuArgs& e, int what, float* out) {
             a.resampled_out = rs.data();
         }
         for (int t = 0; t < T; ++t) {
-            if (packed && (INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC)) {
-                if constexpr (INTERP == INTERP_LINEAR || INTERP == INTERP_CUBIC)
-                    phase_prestage_quad<N, INTERP>(t, reinterpret_cast<const float4*>(spec), cbias, a, v[t].data());
-            } else if (packed)
+            if (packed)
                 phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v[t].data());
             else
                 phase_prestage<N, INTERP>(t, spec, a, v[t].data());
