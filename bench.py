@@ -444,6 +444,7 @@ def batch_bench(dev, seed=3, count=32, steps=20):
     total = sum(s.num_ascans for s, _, _, _ in bufs)
     peak = measured_peak()[0]
     per_len = {}
+    from octproengine_b200.batch import radix_plan
     for n in (1024, 2048, 4096):
         sel = [b for b in bufs if b[0].signal_length == n]
         if not sel:
@@ -451,11 +452,18 @@ def batch_bench(dev, seed=3, count=32, steps=20):
         sub = Batch(items(sel))
         sub.set_tuning(n, tuning[n][0], tuning[n][1])
         ms = timed(lambda: sub.run_graph(sp), steps)
+        # the same buffers as single-buffer launches (each its own chain kernel),
+        # the rate the batch is compared with at this length
+        ms_single = timed(lambda: [c.process_device(x.data_ptr(), o.data_ptr(), sp, num_ascans=s.num_ascans)
+                                   for s, c, x, o in sel], steps)
         nbytes = sum(s.num_ascans * (n * bytes_in[s.input_dtype] + (n // 2) * 4) for s, _, _, _ in sel)
         asc = sum(s.num_ascans for s, _, _, _ in sel)
         per_len[str(n)] = {"buffers": len(sel), "ascans": asc, "ascans_per_s": asc / (ms / 1e3),
                            "gbs": nbytes / (ms / 1e3) / 1e9, "hbm_frac": nbytes / (ms / 1e3) / 1e9 / peak,
-                           "pairs_per_team": tuning[n][0], "radix_schedule": tuning[n][1]}
+                           "single_buffer_launches_ascans_per_s": asc / (ms_single / 1e3),
+                           "batch_over_single": ms_single / ms,
+                           "pairs_per_team": tuning[n][0], "radix_schedule": tuning[n][1],
+                           "radix_plan": radix_plan(n, tuning[n][1])}
         sub.close()
     batch.close()
     for _, c, _, _ in bufs:

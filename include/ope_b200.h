@@ -303,8 +303,10 @@ OPE_B200_API int ope_b200_batch_run(ope_b200_batch* batch, void* stream);
 OPE_B200_API int ope_b200_batch_run_graph(ope_b200_batch* batch, void* stream);
 /* Tuning per signal length n: pairs_per_team (pairs of A-scans each team of
  * N/16 threads takes per grab; a CTA takes 2 x pairs_per_team x 4096/N A-scans)
- * and radix_schedule (0: radix-16 passes then the short one, 1: short first;
- * n = 4096 has only 0). Defaults: 4 and 0. */
+ * and radix_schedule, the FFT radix plan: every pass has radix 16 but one
+ * short pass (radix N / 16^(passes-1)), run last (0), first (1) or second (2):
+ * 1024 = 16*16*4 / 4*16*16 / 16*4*16, 2048 = 16*16*8 / 8*16*16 / 16*8*16;
+ * n = 4096 (16*16*16) has only 0. Defaults: 4 and 0. */
 OPE_B200_API int ope_b200_batch_set_tuning(ope_b200_batch* batch, int32_t n, int32_t pairs_per_team,
                                            int32_t radix_schedule);
 OPE_B200_API int ope_b200_batch_get_tuning(ope_b200_batch* batch, int32_t n, int32_t* pairs_per_team,

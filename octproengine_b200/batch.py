@@ -73,3 +73,11 @@ class Batch:
 
     def autotune(self, reps: int = 3) -> None:
         self._check(capi.lib().ope_b200_batch_autotune(self.h, reps))
+
+
+def radix_plan(n: int, radix_schedule: int) -> str:
+    """The FFT radix plan a schedule runs at length n, e.g. "16x8x16"."""
+    npass = (int(n).bit_length() - 1 + 3) // 4
+    short = n // 16 ** (npass - 1)
+    pos = npass - 1 if radix_schedule == 0 else radix_schedule - 1
+    return "x".join(str(short if p == pos else 16) for p in range(npass))

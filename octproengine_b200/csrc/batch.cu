@@ -114,11 +114,13 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2)
         switch (sd.n) {
             case 1024:
                 if (sd.sched == 0) dispatch_dt_interp<1024, 0>(sd, u, smem);
-                else dispatch_dt_interp<1024, 1>(sd, u, smem);
+                else if (sd.sched == 1) dispatch_dt_interp<1024, 1>(sd, u, smem);
+                else dispatch_dt_interp<1024, 2>(sd, u, smem);
                 break;
             case 2048:
                 if (sd.sched == 0) dispatch_dt_interp<2048, 0>(sd, u, smem);
-                else dispatch_dt_interp<2048, 1>(sd, u, smem);
+                else if (sd.sched == 1) dispatch_dt_interp<2048, 1>(sd, u, smem);
+                else dispatch_dt_interp<2048, 2>(sd, u, smem);
                 break;
             default: dispatch_dt_interp<4096, 0>(sd, u, smem); break;
         }
@@ -146,7 +148,9 @@ int host_team_region(int n, int kind) {
     }
 }
 
-bool has_two_schedules(int n) { return n == 1024 || n == 2048; }
+// Radix plans per length: 1024 = 16*16*4, 4*16*16, 16*4*16; 2048 = 16*16*8,
+// 8*16*16, 16*8*16; 4096 = 16*16*16 (one plan).
+int num_schedules(int n) { return (n == 1024 || n == 2048) ? 3 : 1; }
 
 }  // namespace ope_b200
 
@@ -208,7 +212,7 @@ int prepare(ope_b200_batch* b, const std::vector<int>& pick, BatchDesc** dst, in
         BatchDesc d = b->base[i];
         const auto tn = b->tuning.count(d.n) ? b->tuning[d.n] : std::make_pair(4, 0);
         d.pairs_per_team = tn.first;
-        d.sched = has_two_schedules(d.n) ? tn.second : 0;
+        d.sched = tn.second < num_schedules(d.n) ? tn.second : 0;
         d.a.tw = b->tw[{d.n, d.sched}];
         const long long npairs = (d.a.m + 1) / 2;
         const long long per_unit = (long long)d.pairs_per_team * d.teams;
@@ -305,7 +309,7 @@ int ope_b200_batch_create(const ope_b200_batch_item* items, int32_t count, ope_b
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->last_launch, cudaEventDisableTiming);
     for (const BatchDesc& d : b->base)
-        for (int s = 0; s < (has_two_schedules(d.n) ? 2 : 1) && e == cudaSuccess; ++s) {
+        for (int s = 0; s < num_schedules(d.n) && e == cudaSuccess; ++s) {
             if (b->tw.count({d.n, s})) continue;
             const std::vector<float2> t = build_twiddles(d.n, s);
             float2* p = nullptr;
@@ -338,10 +342,11 @@ const char* ope_b200_batch_last_error(const ope_b200_batch* b) { return b ? b->e
 
 int ope_b200_batch_set_tuning(ope_b200_batch* b, int32_t n, int32_t pairs_per_team, int32_t radix_schedule) {
     if (!b) return OPE_B200_E_INVALID;
-    if (pairs_per_team < 1 || pairs_per_team > 1024 || radix_schedule < 0 || radix_schedule > 1)
-        return bfail(b, OPE_B200_E_INVALID, "pairs_per_team must be in [1, 1024] and radix_schedule 0 or 1");
-    if (radix_schedule == 1 && !has_two_schedules(n))
-        return bfail(b, OPE_B200_E_INVALID, "this length has a single radix schedule");
+    if (pairs_per_team < 1 || pairs_per_team > 1024 || radix_schedule < 0)
+        return bfail(b, OPE_B200_E_INVALID, "pairs_per_team must be in [1, 1024] and radix_schedule >= 0");
+    if (radix_schedule >= num_schedules(n))
+        return bfail(b, OPE_B200_E_INVALID, "radix_schedule out of range for this length (0..2 at 1024 and 2048, "
+                                             "0 at 4096)");
     b->tuning[n] = {pairs_per_team, radix_schedule};
     drop_graph(b);
     return OPE_B200_OK;
@@ -405,7 +410,7 @@ int ope_b200_batch_autotune(ope_b200_batch* b, int32_t reps) {
         const int n = kv.first;
         float best = 1e30f;
         std::pair<int, int> best_cfg{4, 0};
-        for (int sched = 0; sched < (has_two_schedules(n) ? 2 : 1) && rc == OPE_B200_OK; ++sched)
+        for (int sched = 0; sched < num_schedules(n) && rc == OPE_B200_OK; ++sched)
             for (int pp : kPairs) {
                 b->tuning[n] = {pp, sched};
                 rc = launch(b, kv.second, s);  // warm-up

@@ -377,8 +377,10 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
         fft_twiddle_dft<N, NPASS - 1, false, S>(t, v, a.tw);
         const long long ra = row0 + 2 * item;
         sink(t, v, ra, ra + 1 < row_end, dc);
-        tm.sync();  // next item overwrites spec/exch
+        // the next item's writes to spec/exch come after the barrier at the top
+        // of the loop, which every thread reaches only once its sink is done
     }
+    tm.sync();  // the caller may reuse the region once the last item's loads are done
 }
 
 template <int N, int S, class Team>

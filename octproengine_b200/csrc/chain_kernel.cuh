@@ -795,15 +795,16 @@ OPE_HD void phase_prestage_packed(int t, const uint32_t* specw, float2 cbias, co
 // q to (d - k)*R + k + q*NS.
 //
 // Radix schedule S: every pass has radix 16 except one of radix LASTR
-// (N = 16^(NPASS-1) * LASTR); S = 0 runs that pass last, S = 1 first.
+// (N = 16^(NPASS-1) * LASTR); S = 0 runs that pass last, S >= 1 runs it as
+// pass S - 1 (S = 1: first; S = 2: second, e.g. 16*8*16 at N = 2048).
+OPE_HD constexpr int short_pass_of(int npass, int s) { return s == 0 ? npass - 1 : s - 1; }
 
 template <int N, int S>
 struct Sched {
-    static_assert(S == 0 || S == 1, "radix schedule 0 (small radix last) or 1 (small radix first)");
     static constexpr int NPASS = Plan<N>::NPASS;
-    static constexpr int radix(int p) {
-        return (S == 0) ? ((p == NPASS - 1) ? Plan<N>::LASTR : 16) : ((p == 0) ? Plan<N>::LASTR : 16);
-    }
+    static_assert(S >= 0 && (S == 0 || S - 1 < NPASS), "radix schedule: 0 (short pass last) or 1 + its pass index");
+    static constexpr int SHORT = short_pass_of(NPASS, S);
+    static constexpr int radix(int p) { return p == SHORT ? Plan<N>::LASTR : 16; }
     static constexpr int span(int p) {
         int v = 1;
         for (int q = 0; q < p; ++q) v *= radix(q);

@@ -41,7 +41,7 @@ std::vector<float2> build_twiddles(int n, int sched) {
     // Per Stockham pass p >= 1 (radix R, span NS): (R-1) x NS entries,
     // entry (r-1)*NS + k = W_N^(r k N/(NS R)), matching Sched::tw_off.
     // Every pass has radix 16 except one of radix lastr, run last (sched 0)
-    // or first (sched 1).
+    // or as pass sched - 1 (sched >= 1).
     std::vector<float2> tw(n, make_float2(1.0f, 0.0f));
     int log2n = 0;
     while ((1 << log2n) < n) ++log2n;
@@ -49,7 +49,7 @@ std::vector<float2> build_twiddles(int n, int sched) {
     const int lastr = 1 << (log2n - 4 * (npass - 1));
     int off = 0, ns = 1;
     for (int p = 0; p < npass; ++p) {
-        const int r_p = (sched == 0) ? ((p == npass - 1) ? lastr : 16) : ((p == 0) ? lastr : 16);
+        const int r_p = (p == short_pass_of(npass, sched)) ? lastr : 16;
         if (p > 0) {
             const int stride = n / (ns * r_p);
             for (int r = 1; r < r_p; ++r)

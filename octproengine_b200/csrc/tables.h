@@ -13,7 +13,8 @@ namespace ope_b200 {
 // evaluated with the same float operations.
 float lanczos8(float x);
 
-// Twiddles of the Stockham passes of radix schedule `sched` (Sched<N, S>),
+// Twiddles of the Stockham passes of radix schedule `sched` (Sched<N, S>: the
+// short pass last for 0, as pass sched - 1 otherwise),
 // per pass a block of (R-1) x NS entries W_N^(r k N/(NS R)) (see
 // Sched::tw_off), evaluated in double and rounded once.
 std::vector<float2> build_twiddles(int n, int sched = 0);

@@ -107,14 +107,17 @@ def test_every_unit_size_gives_the_same_bits(cuda, pairs):
         assert np.array_equal(g, r)
 
 
-def test_short_radix_first_schedule_matches_oracle(cuda):
+@pytest.mark.parametrize("sched", [1, 2])
+def test_other_radix_schedules_match_oracle(cuda, sched):
+    """Radix plans with the short pass first (4*16*16, 8*16*16) or second
+    (16*4*16, 16*8*16): a different evaluation order, as accurate."""
     from octproengine_b200.batch import Batch
     specs = [_spec(n, 37, UINT16, CUBIC, HANN, 5 + n) for n in (1024, 2048)]
     bufs = _Bufs(specs, cuda, seed=20)
     ref = bufs.single()
     with Batch(bufs.items()) as b:
-        b.set_tuning(1024, 2, 1)
-        b.set_tuning(2048, 2, 1)
+        b.set_tuning(1024, 2, sched)
+        b.set_tuning(2048, 2, sched)
         b.run(_stream())
         got = bufs.outputs()
     for s, g, r, raw in zip(specs, got, ref, bufs.raw):
@@ -158,7 +161,7 @@ def test_autotune_picks_a_candidate_and_keeps_results(cuda):
         b.autotune(reps=2)
         for n in (1024, 2048, 4096):
             pp, sc, us = b.tuning(n)
-            assert pp in (1, 2, 4, 8, 16, 32) and sc in (0, 1) and us > 0
+            assert pp in (1, 2, 4, 8, 16, 32) and sc in (0, 1, 2) and us > 0
             if n == 4096:
                 assert sc == 0
         b.run(_stream())
@@ -204,6 +207,8 @@ def test_batch_rejects_what_it_cannot_run(cuda):
     with Batch([(ctx, d.data_ptr(), o.data_ptr(), 4)]) as b:
         with pytest.raises(capi.B200Error):
             b.set_tuning(4096, 4, 1)  # 4096 has one schedule
+        with pytest.raises(capi.B200Error):
+            b.set_tuning(2048, 4, 3)  # three plans at 2048
         with pytest.raises(capi.B200Error):
             b.set_tuning(2048, 0, 0)
 
