@@ -367,6 +367,8 @@ def autofocus_bench(dev, seeds=range(8), ascans=1024):
             "seconds_median": med("joint_fit_s"), "evaluations_median": med("joint_fit_evals"),
             "error_dispersion_median": med("joint_fit_err_dispersion"), "error_kmap_median": med("joint_fit_err_kmap"),
             "error_max": float(max(jw)), "trials_within_1pct": int(sum(e < 0.01 for e in jw)),
+            "trials_kmap_within_1pct": int(sum(t["joint_fit_err_kmap"] < 0.01 for t in trials)),
+            "trials_within_3pct": int(sum(e < 0.03 for e in jw)),
             "speedup_vs_sweep_median": float(np.median([t["sweep_s"] / t["joint_fit_s"] for t in trials])),
             "sweep_at_nominal_kmap_error_median": med("sweep_nominal_kmap_err"),
         },
