@@ -240,6 +240,11 @@ typedef struct ope_b200_af ope_b200_af;
 OPE_B200_API int ope_b200_af_create(int32_t n, int32_t input_dtype, int32_t interpolation, const float* window,
                                     int32_t device, ope_b200_af** out);
 OPE_B200_API void ope_b200_af_destroy(ope_b200_af* af);
+/* DataParameters::bitshift for the fit's data: with `on`, every 8- or 16-bit
+ * sample is shifted right by 4 before the chain, in the forward and the
+ * adjoint alike, as the processing chain does with the flag set, so a fit
+ * sharpens the image the chain will produce. Ignored for float32 input. */
+OPE_B200_API int ope_b200_af_set_bitshift(ope_b200_af* af, int32_t on);
 OPE_B200_API const char* ope_b200_af_last_error(const ope_b200_af* af);
 /* Forward over num_ascans A-scans at d_in (16-byte aligned). d_out (may be
  * NULL): num_ascans x N/2 floats in `output_mode`. d_hs (may be NULL): two

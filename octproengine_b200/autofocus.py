@@ -97,7 +97,7 @@ class Autofocus:
     at a time (its device tables and partial sums are shared by its calls)."""
 
     def __init__(self, n: int, input_dtype: str = "uint16", interpolation: int = LANCZOS,
-                 window: Optional[np.ndarray] = None, device: int = 0):
+                 window: Optional[np.ndarray] = None, device: int = 0, bitshift: bool = False):
         if input_dtype not in _DTYPES:
             raise ValueError(f"input_dtype must be one of {sorted(_DTYPES)}")
         self.n = int(n)
@@ -116,6 +116,8 @@ class Autofocus:
         if rc != capi.OK:
             raise capi.B200Error(rc, f"autofocus handle for N={n}, {input_dtype}, interpolation {interpolation}")
         self.h = h
+        if bitshift:  # DataParameters::bitshift: 8/16-bit samples >> 4, as the chain applies it
+            self._check(capi.lib().ope_b200_af_set_bitshift(self.h, 1))
 
     def close(self) -> None:
         if getattr(self, "h", None):

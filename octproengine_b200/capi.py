@@ -121,6 +121,7 @@ SIGNATURES = {
     "ope_b200_af_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _FP, ctypes.c_int32,
                                            ctypes.POINTER(_P)]),
     "ope_b200_af_destroy": (None, [_P]),
+    "ope_b200_af_set_bitshift": (ctypes.c_int, [_P, ctypes.c_int32]),
     "ope_b200_af_last_error": (ctypes.c_char_p, [_P]),
     "ope_b200_af_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P]),
     "ope_b200_af_backward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, ctypes.c_int32, _P, _P, _P, _P]),

@@ -168,6 +168,7 @@ struct ope_b200_af {
     double* partial = nullptr;
     int cap = 0;
     const float* tables_params = nullptr;  // parameter pointer the device tables were last built from
+    int bitshift = 0;  // 8/16-bit samples >> 4 before the chain (DataParameters::bitshift)
     std::string err;
 };
 
@@ -242,6 +243,7 @@ int af_prepare(ope_b200_af* o, const void* d_in, int64_t num_ascans, const float
     a.c.dc_resp = o->dc_zero;  // integer-mean split, nothing added back
     a.c.timeout_ns = 2000000000ull;
     a.c.neg_zero = -0.0f;
+    a.c.bitshift = o->bitshift;
     a.lz_dw = o->lzdw;
     a.rmask = o->rmask;
     a.partial = o->partial;
@@ -262,6 +264,12 @@ __global__ void af_small_copy_kernel(unsigned char* dst, const unsigned char* sr
 }
 
 extern "C" {
+
+int ope_b200_af_set_bitshift(ope_b200_af* af, int32_t on) {
+    if (!af) return OPE_B200_E_INVALID;
+    af->bitshift = (on && (af->in_kind == IN_U8 || af->in_kind == IN_U16)) ? 1 : 0;
+    return OPE_B200_OK;
+}
 
 int ope_b200_af_create(int32_t n, int32_t input_dtype, int32_t interpolation, const float* window, int32_t device,
                        ope_b200_af** out) {

@@ -292,6 +292,12 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
             }
         }
         __syncthreads();
+        if constexpr (DT == IN_U8 || DT == IN_U16) {
+            if (c.bitshift) {  // as the forward applies it (run_pairs)
+                phase_bitshift<N, DT>(t, stage);
+                __syncthreads();
+            }
+        }
         // ---- x - c (exact integer mean) ----
         {
             float2 vals[16];

@@ -284,6 +284,29 @@ def test_joint_fit_recovers_dispersion_and_kmap_from_the_nominal_kmap(cuda):
 
 
 @pytest.mark.gpu
+def test_bitshift_applies_to_forward_and_adjoint(cuda):
+    """With the bitshift flag the fit works on the samples >> 4, as the chain
+    does (DataParameters::bitshift): entropy and all 8 gradient entries equal
+    those of an unshifted handle given the data shifted on the host."""
+    from octproengine_b200.autofocus import Autofocus
+    raw_t, raw, window, ctrue = make_case(m=64, seed=41)
+    shifted = torch.from_numpy((raw >> 4).astype(np.uint16).view(np.int16).copy())
+    p = torch.from_numpy(params_of(8.0, -3.0, ctrue)).to(cuda)
+    res = []
+    for data, flag in ((raw_t, True), (shifted, False)):
+        af = Autofocus(N, "uint16", O.LANCZOS, window=window, bitshift=flag)
+        d = data.to(cuda).contiguous()
+        hs = torch.empty(2, dtype=torch.float64, device=cuda)
+        g = torch.empty(8, dtype=torch.float32, device=cuda)
+        af.forward(d, p, hs=hs)
+        af.backward(d, p, g, hs=hs)
+        torch.cuda.synchronize()
+        res.append((hs.cpu().numpy(), g.cpu().numpy()))
+        af.close()
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+@pytest.mark.gpu
 def test_reused_evaluator_serves_new_data_like_a_fresh_one(cuda):
     from octproengine_b200.autofocus import FitEvaluator, fit_dispersion
     cases = [make_case(m=128, seed=s, d2=d2, d3=d3) for s, d2, d3 in ((21, 15.0, -8.0), (22, -25.0, 6.0))]
