@@ -45,3 +45,18 @@ def test_reference_arm_loads_nothing_of_the_package(reflib):
     sys.path.insert(0, ROOT)
     import bench
     assert line["config"] == json.loads(json.dumps(bench.bench_config(1)))
+
+
+def test_kernel_counters_file_feeds_the_roofline_fields():
+    """profiles/chain_kernel_n2048_cubic_u16.json (an ncu capture of one chain
+    launch) holds what the bench line's roofline.traffic and fp32_pipe quote:
+    the captured A-scan count, DRAM bytes near the algorithmic 4096 B read per
+    A-scan, the pipe counters and the command that made it."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.kernel_counters()
+    assert c is not None and c["ascans"] > 0 and c["command"].startswith("ncu ")
+    read_per_ascan = c["dram_bytes_read"] / c["ascans"]
+    assert 4096 <= read_per_ascan < 4096 * 1.05
+    for k in ("fma_pipe_active_pct", "issue_active_pct", "warps_active_pct", "thread_inst_per_ascan"):
+        assert c[k] > 0
