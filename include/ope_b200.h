@@ -343,8 +343,9 @@ OPE_B200_API int ope_b200_op_klinearization(const float* input, const float* cur
 OPE_B200_API int ope_b200_op_window_dispersion(const float* input, const float* window, const float* phase_cos_sin,
                                                int32_t mode, int32_t line_width, int64_t samples, float* out);
 /* |DFT| of one real line, all line_width outputs: inverse = 1 is the reference's
- * ifft (unnormalised exp(+i), cpu_backend.cpp:634-659), 0 the forward transform;
- * evaluated in double. */
+ * ifft (unnormalised exp(+i), cpu_backend.cpp:634-659), 0 the forward transform
+ * (the same magnitudes for a real line). Power-of-two lengths 512..8192 run the
+ * chain's own float32 Stockham FFT; other lengths a direct DFT in double. */
 OPE_B200_API int ope_b200_op_dft_magnitude(const float* input, int32_t line_width, int32_t inverse, float* out);
 /* getMinimumVarianceMean over height rows of width interleaved complex values:
  * 2*width floats (cpu_kernels.tpp:402-458, same double accumulation). */

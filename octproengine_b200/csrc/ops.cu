@@ -19,6 +19,7 @@
 #include "../../include/ope_b200.h"
 #include "autofocus.cuh"
 #include "postproc.h"
+#include "tables.h"
 
 namespace ope_b200 {
 namespace {
@@ -105,6 +106,62 @@ __global__ void op_dft_mag_kernel(const float* in, int n, double sign, float* ou
     }
     const float fr = (float)re, fi = (float)im;
     out[k] = __fsqrt_rn(__fadd_rn(__fmul_rn(fr, fr), __fmul_rn(fi, fi)));
+}
+
+// The same magnitudes through the chain's own FFT for power-of-two lengths
+// 512..8192: one team of N/16 threads runs the Stockham radix-16 passes of the
+// fused kernel (fft_twiddle_dft, every output of the last pass) on the line in
+// lane a of the packed pairs. For a real line |DFT^-(x)| = |DFT^+(x)| (the two
+// transforms are complex conjugates), so both directions use the exp(+i) one.
+template <int N>
+__global__ void __launch_bounds__(N / 16) op_fft_mag_kernel(const float* in, const float2* tw, float* out) {
+    extern __shared__ __align__(16) unsigned char op_smem[];
+    float4* exch = reinterpret_cast<float4*>(op_smem);
+    constexpr int T = N / 16;
+    constexpr int NPASS = Plan<N>::NPASS;
+    const int t = threadIdx.x;
+    cp v[16];
+#pragma unroll
+    for (int s = 0; s < 16; ++s) v[s] = cpmake(make_float2(in[t + s * T], 0.0f), make_float2(0.0f, 0.0f));
+    fft_twiddle_dft<N, 0, NPASS == 1>(t, v, tw);
+    if constexpr (NPASS > 1) {
+        fft_store<N, 0>(t, v, exch);
+        __syncthreads();
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, 1, NPASS == 2>(t, v, tw);
+    }
+    if constexpr (NPASS > 2) {
+        __syncthreads();
+        fft_store<N, 1>(t, v, exch);
+        __syncthreads();
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, 2, NPASS == 3>(t, v, tw);
+    }
+    if constexpr (NPASS > 3) {
+        __syncthreads();
+        fft_store<N, 2>(t, v, exch);
+        __syncthreads();
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, 3, true>(t, v, tw);
+    }
+    using PI = PassInfo<N, NPASS - 1>;
+#pragma unroll
+    for (int i = 0; i < PI::D; ++i)
+#pragma unroll
+        for (int q = 0; q < PI::R; ++q) {
+            const cp x = v[i + q * PI::D];
+            out[t + i * T + q * (N / PI::R)] =
+                __fsqrt_rn(__fadd_rn(__fmul_rn(x.re.x, x.re.x), __fmul_rn(x.im.x, x.im.x)));
+        }
+}
+
+template <int N>
+cudaError_t launch_fft_mag(const float* d_in, const float2* d_tw, float* d_out) {
+    constexpr int SMEM = Plan<N>::EXCH_ELEMS * 16;
+    cudaError_t e = cudaFuncSetAttribute(op_fft_mag_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    op_fft_mag_kernel<N><<<1, N / 16, SMEM>>>(d_in, d_tw, d_out);
+    return cudaGetLastError();
 }
 
 // getMinimumVarianceMean (cpu_kernels.tpp:402-458), one thread per column,
@@ -312,7 +369,22 @@ int ope_b200_op_dft_magnitude(const float* input, int32_t line_width, int32_t in
     float *d_in, *d_out;
     OPS_CU(s.upload(&d_in, input, line_width * sizeof(float)));
     OPS_CU(s.alloc(&d_out, line_width * sizeof(float)));
-    op_dft_mag_kernel<<<(line_width + 127) / 128, 128>>>(d_in, line_width, inverse ? 1.0 : -1.0, d_out);
+    const int n = line_width;
+    if (n >= 512 && n <= 8192 && (n & (n - 1)) == 0) {
+        // the chain's FFT (float32, its twiddle table)
+        const std::vector<float2> tw = build_twiddles(n);
+        float2* d_tw;
+        OPS_CU(s.upload(&d_tw, tw.data(), tw.size() * sizeof(float2)));
+        cudaError_t e = n == 512    ? launch_fft_mag<512>(d_in, d_tw, d_out)
+                        : n == 1024 ? launch_fft_mag<1024>(d_in, d_tw, d_out)
+                        : n == 2048 ? launch_fft_mag<2048>(d_in, d_tw, d_out)
+                        : n == 4096 ? launch_fft_mag<4096>(d_in, d_tw, d_out)
+                                    : launch_fft_mag<8192>(d_in, d_tw, d_out);
+        OPS_CU(e);
+    } else {
+        // any other length: a direct DFT evaluated in double
+        op_dft_mag_kernel<<<(n + 127) / 128, 128>>>(d_in, n, inverse ? 1.0 : -1.0, d_out);
+    }
     return finish(d_out, out, line_width);
 }
 
