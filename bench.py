@@ -394,7 +394,9 @@ def batch_bench(dev, seed=3, count=32, steps=20):
     on, log output. The autotuner picks pairs-per-team and the radix schedule
     per length first. Reported: total A-scans/s of the one-launch batch, the
     same buffers as sequential single-buffer launches, and per length the HBM
-    fraction of that length's buffers launched alone.
+    fraction of that length's buffers launched alone, beside the rate those
+    buffers would reach at the single-buffer kernel's steady rate for each
+    buffer's configuration (input type, resampling; one long launch each).
     """
     import torch
     from octproengine_b200 import synth
@@ -458,12 +460,25 @@ def batch_bench(dev, seed=3, count=32, steps=20):
         # the rate the batch is compared with at this length
         ms_single = timed(lambda: [c.process_device(x.data_ptr(), o.data_ptr(), sp, num_ascans=s.num_ascans)
                                    for s, c, x, o in sel], steps)
+        # each buffer's own configuration at the single-buffer kernel's steady
+        # rate: one launch over >= 32768 A-scans of it (its rows repeated), so
+        # the time these buffers would take at that rate is sum(m_i / rate_i)
+        ms_steady = 0.0
+        for s, c, x, _ in sel:
+            reps_rows = -(-32768 // s.num_ascans)
+            xb = x.repeat(reps_rows, 1)
+            ob = torch.empty((xb.shape[0], n // 2), dtype=torch.float32, device=dev)
+            ms_big = timed(lambda: c.process_device(xb.data_ptr(), ob.data_ptr(), sp, num_ascans=xb.shape[0]), 5)
+            ms_steady += ms_big * s.num_ascans / xb.shape[0]
+            del xb, ob
         nbytes = sum(s.num_ascans * (n * bytes_in[s.input_dtype] + (n // 2) * 4) for s, _, _, _ in sel)
         asc = sum(s.num_ascans for s, _, _, _ in sel)
         per_len[str(n)] = {"buffers": len(sel), "ascans": asc, "ascans_per_s": asc / (ms / 1e3),
                            "gbs": nbytes / (ms / 1e3) / 1e9, "hbm_frac": nbytes / (ms / 1e3) / 1e9 / peak,
                            "single_buffer_launches_ascans_per_s": asc / (ms_single / 1e3),
                            "batch_over_single": ms_single / ms,
+                           "single_kernel_steady_ascans_per_s": asc / (ms_steady / 1e3),
+                           "batch_over_steady": ms_steady / ms,
                            "pairs_per_team": tuning[n][0], "radix_schedule": tuning[n][1],
                            "radix_plan": radix_plan(n, tuning[n][1])}
         sub.close()

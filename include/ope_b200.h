@@ -306,18 +306,20 @@ OPE_B200_API int ope_b200_batch_run(ope_b200_batch* batch, void* stream);
  * change) captures it, later calls replay it. The graph keeps the buffer
  * pointers of the batch. */
 OPE_B200_API int ope_b200_batch_run_graph(ope_b200_batch* batch, void* stream);
-/* Tuning per signal length n: pairs_per_team (pairs of A-scans each team of
- * N/16 threads takes per grab; a CTA takes 2 x pairs_per_team x 4096/N A-scans)
+/* Tuning per signal length n: pairs_per_team (pairs of A-scans a team of
+ * N/16 threads takes from its length's work counter per grab; the team stages
+ * the next pair while computing the current one across grabs and buffers, so
+ * the grab size only trades counter traffic against the balance at the end)
  * and radix_schedule, the FFT radix plan: every pass has radix 16 but one
  * short pass (radix N / 16^(passes-1)), run last (0), first (1) or second (2):
  * 1024 = 16*16*4 / 4*16*16 / 16*4*16, 2048 = 16*16*8 / 8*16*16 / 16*8*16;
- * n = 4096 (16*16*16) has only 0. Defaults: 4 and 0. */
+ * n = 4096 (16*16*16) has only 0. Defaults: 2 and 0. */
 OPE_B200_API int ope_b200_batch_set_tuning(ope_b200_batch* batch, int32_t n, int32_t pairs_per_team,
                                            int32_t radix_schedule);
 OPE_B200_API int ope_b200_batch_get_tuning(ope_b200_batch* batch, int32_t n, int32_t* pairs_per_team,
                                            int32_t* radix_schedule, float* best_us);
 /* Autotuner: for every length in the batch, times each candidate
- * (pairs_per_team in {1, 2, 4, 8, 16, 32} x the radix schedules) on the
+ * (pairs_per_team in {1, 2, 4, 8} x the radix schedules) on the
  * batch's own buffers of that length (`reps` timed launches each, CUDA
  * events, best kept) and keeps the fastest. Overwrites the outputs. */
 OPE_B200_API int ope_b200_batch_autotune(ope_b200_batch* batch, int32_t reps);

@@ -8,19 +8,27 @@
 // described by an ope_b200_ctx (its ProcessorConfiguration and curves), so
 // every buffer gets exactly the chain a single-buffer call would run.
 //
-// Work decomposition. A CTA has 256 threads; a buffer of N samples per A-scan
-// is processed by teams of N/16 threads (4096/N teams per CTA, each with its
-// own named barrier and shared-memory region), every team running the same
-// pair-of-A-scans pipeline as the single-buffer kernel (run_pairs). The
-// buffers' A-scan pairs are cut into units of teams x pairs_per_team pairs;
-// persistent CTAs take units from a global counter (the last CTA to finish
-// resets it, so a captured graph replays without a memset). The autotuner
-// picks pairs_per_team (the A-scans each CTA takes per grab) and the FFT radix
-// schedule per length by timing this batch's own buffers of that length.
+// Work decomposition. The buffers are grouped by length N; a group's A-scan
+// pairs are numbered consecutively over its buffers. A CTA has 256 threads
+// and, while it works on a group, runs 4096/N teams of N/16 threads (each
+// with its own named barrier and shared-memory region laid out for the
+// widest input type), every team running the single-buffer kernel's
+// pair-of-A-scans pipeline (pair_unpack, pair_prestage, pair_fft, the image
+// epilogue) with the input type and resampling mode of each pair's buffer
+// chosen at run time. Teams take pairs from the group's counter in grabs of
+// `chunk` pairs and stage the next pair (of any buffer of the group) while
+// computing the current one, so the copy/compute pipeline runs unbroken
+// across grabs and buffers. Each CTA starts on the group whose CTA range
+// (proportional to the group's estimated work) holds it and then visits the
+// other groups in turn, entering only those with pairs left; the last CTA to
+// finish resets the counters, so a captured graph replays without a memset.
+// The autotuner picks the grab size and the FFT radix schedule per length by
+// timing this batch's own buffers of that length.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <map>
 #include <string>
 #include <vector>
@@ -35,117 +43,219 @@ int ctx_batch_args(ope_b200_ctx* c, ChainArgs* a, int* n, int* in_kind, int* int
 const char* ctx_error(const ope_b200_ctx* c);
 
 constexpr int BATCH_THREADS = 256;
+constexpr int BATCH_MAX_GROUPS = 3;  // one per supported length
 
 struct BatchDesc {
     ChainArgs a;
-    int n, in_kind, interp, sched;
-    int teams;           // teams of n/16 threads per CTA
-    int pairs_per_team;  // pairs each team takes per unit
-    int region;          // bytes of shared memory per team
-    int pad;
-    long long unit0, units;  // this buffer's units in the global numbering
+    int n, in_kind, interp, group;
+    long long pair0;   // first pair of this buffer in its group's numbering
+    long long npairs;  // (m + 1) / 2
 };
 
-template <int N, int DT>
-constexpr int team_region() {
-    return ((Layout<N, DT>::TOTAL + 127) / 128) * 128;
+struct GroupDesc {
+    int n, sched;
+    int first;          // index of the group's first descriptor (its buffers are consecutive)
+    int count;
+    long long npairs;   // pairs of all the group's buffers
+    int chunk;          // pairs per grab
+    int cta_begin;      // first CTA that starts on this group
+};
+
+// One team's region: Layout<N, IN_F32> (the widest stage); the spectrum,
+// prefix, scan and exchange offsets are the same for 8-, 16-bit and float
+// samples, so pair_unpack<N, DT> of any of them works in it.
+template <int N>
+struct BatchRegion {
+    using LY = Layout<N, IN_F32>;
+    static_assert(Layout<N, IN_U8>::OFF_STAGE == LY::OFF_STAGE && Layout<N, IN_U16>::OFF_STAGE == LY::OFF_STAGE &&
+                      Layout<N, IN_U8>::OFF_SCAN == LY::OFF_SCAN && Layout<N, IN_U16>::OFF_SCAN == LY::OFF_SCAN &&
+                      Layout<N, IN_U8>::OFF_PFX == LY::OFF_PFX && Layout<N, IN_U16>::OFF_PFX == LY::OFF_PFX,
+                  "batched teams share one layout for every input type");
+    static constexpr int BYTES = ((LY::TOTAL + 127) / 128) * 128;
+    static constexpr int TEAMS = BATCH_THREADS / (N / 16);
+};
+
+// Team control words after a team's mbarrier (Layout::OFF_MBAR, 64 bytes):
+// the abort flag, the staged pair (descriptor, pair within its buffer) and
+// thread 0's grab [lo, hi) and descriptor cursor.
+struct TeamCtl {
+    uint64_t mbar;
+    int pad0, pad1;
+    int abort;
+    int next_desc;  // -1: no further pair
+    long long next_pair;
+    long long grab_lo, grab_hi;
+    int cursor;
+    int pad2;
+};
+static_assert(sizeof(TeamCtl) <= 64, "team control words fit the mbarrier slot");
+
+__device__ __forceinline__ uint32_t in_bytes(int kind) { return kind == IN_U8 ? 1u : kind == IN_U16 ? 2u : 4u; }
+
+// Thread 0 of a team: takes the team's next pair of group g (a new grab of
+// g.chunk pairs from `counter` when the current one is used up), publishes it
+// in the control words and issues the copy of its rows into the stage; or
+// publishes "none". A team's pairs only increase, so the descriptor cursor
+// only moves forward.
+template <int N>
+__device__ __noinline__ void team_stage_next(const BatchDesc* __restrict__ descs, const GroupDesc* g,
+                                             unsigned long long* counter, unsigned char* my) {
+    using LY = typename BatchRegion<N>::LY;
+    TeamCtl* c = reinterpret_cast<TeamCtl*>(my + LY::OFF_MBAR);
+    if (c->grab_lo >= c->grab_hi) {
+        const long long s = (long long)atomicAdd(counter, (unsigned long long)g->chunk);
+        if (s >= g->npairs) {
+            c->next_desc = -1;
+            return;
+        }
+        c->grab_lo = s;
+        c->grab_hi = (s + g->chunk < g->npairs) ? s + g->chunk : g->npairs;
+    }
+    const long long p = c->grab_lo++;
+    int di = c->cursor;
+    while (descs[di].pair0 + descs[di].npairs <= p) ++di;
+    c->cursor = di;
+    const BatchDesc& D = descs[di];
+    const long long lp = p - D.pair0;
+    const long long r = 2 * lp;
+    const uint32_t row_bytes = (uint32_t)N * in_bytes(D.in_kind);
+    const uint32_t bytes = ((D.a.m - r) >= 2 ? 2u : 1u) * row_bytes;
+    c->next_desc = di;
+    c->next_pair = lp;
+    fence_proxy_async_smem();
+    mbar_expect_tx(&c->mbar, bytes);
+    bulk_g2s(my + LY::OFF_STAGE, static_cast<const unsigned char*>(D.a.in) + r * (long long)row_bytes, bytes,
+             &c->mbar);
 }
 
-template <int N, int DT, int INTERP, int S>
-__device__ __noinline__ void batch_team_run(const BatchDesc& d, long long u, unsigned char* smem) {
+// One team's share of group g: the pairs team_stage_next hands it, one at a
+// time through the pipeline, the next pair's copy issued as soon as the
+// current pair's rows are unpacked. Returns whether a bounded wait ran out
+// (the team stops; the status word says so).
+template <int N, int S>
+__device__ __forceinline__ bool group_run(const BatchDesc* __restrict__ descs, const GroupDesc* g,
+                                          unsigned long long* counter, unsigned char* smem) {
+    using R = BatchRegion<N>;
+    using LY = typename R::LY;
     constexpr int T = N / 16;
     const int team = threadIdx.x / T;
-    if (team >= d.teams) return;
     const SubTeam tm{team * T, 1 + team, T};
-    unsigned char* my = smem + team * d.region;
-    const long long npairs = (d.a.m + 1) / 2;
-    const long long per_unit = (long long)d.pairs_per_team * d.teams;
-    const long long p0 = (u - d.unit0) * per_unit;
-    const long long p_end = (p0 + per_unit < npairs) ? p0 + per_unit : npairs;
-    ImageSink<N, S, SubTeam> sink{tm, d.a, reinterpret_cast<float*>(my + Layout<N, DT>::OFF_SCAN)};
-    run_pairs<N, DT, INTERP, S>(tm, d.a, 0, d.a.m, p0 + team, p_end, d.teams, my, sink);
+    unsigned char* my = smem + team * R::BYTES;
+    TeamCtl* ctl = reinterpret_cast<TeamCtl*>(my + LY::OFF_MBAR);
+    const int t = tm.tid();
+    if (t == 0) {
+        mbar_init(&ctl->mbar, 1);
+        fence_mbar_init();
+        ctl->abort = 0;
+        ctl->grab_lo = ctl->grab_hi = 0;
+        ctl->cursor = g->first;
+        team_stage_next<N>(descs, g, counter, my);
+    }
     tm.sync();
-    if (tm.tid() == 0) {  // the region may hold another layout in the next unit
-        uint64_t* mbar = reinterpret_cast<uint64_t*>(my + Layout<N, DT>::OFF_MBAR);
-        mbar_inval(&mbar[0]);
+    for (int it = 0;; ++it) {
+        const int cd = ctl->next_desc;
+        if (cd < 0) break;
+        const long long lp = ctl->next_pair;
+        const ChainArgs& a = descs[cd].a;
+        const bool ok = mbar_wait_bounded(&ctl->mbar, it & 1, a.timeout_ns);
+        if (!ok) ctl->abort = 1;
+        tm.sync();
+        if (ctl->abort) {
+            // as run_pairs: wait out the copy of this phase (a second bound) before leaving
+            if (t == 0) {
+                int st = STATUS_MBAR_TIMEOUT;
+                if (!mbar_wait_bounded(&ctl->mbar, it & 1, a.timeout_ns)) st |= STATUS_COPY_PENDING;
+                if (a.status) atomicOr(a.status, st);
+            }
+            break;
+        }
+        float2 dc, cbias;
+        bool packed;
+        const int kind = descs[cd].in_kind;
+        if (kind == IN_U8) packed = pair_unpack<N, IN_U8>(tm, t, a, my, dc, cbias);
+        else if (kind == IN_U16) packed = pair_unpack<N, IN_U16>(tm, t, a, my, dc, cbias);
+        else packed = pair_unpack<N, IN_F32>(tm, t, a, my, dc, cbias);
+        tm.sync();
+        // every thread is done with the stage and has read next_*
+        if (t == 0) team_stage_next<N>(descs, g, counter, my);
+        cp v[16];
+        const int interp = descs[cd].interp;
+        if (interp == INTERP_CUBIC) pair_prestage<N, INTERP_CUBIC>(t, packed, my, cbias, a, v);
+        else if (interp == INTERP_LINEAR) pair_prestage<N, INTERP_LINEAR>(t, packed, my, cbias, a, v);
+        else if (interp == INTERP_LANCZOS) pair_prestage<N, INTERP_LANCZOS>(t, packed, my, cbias, a, v);
+        else pair_prestage<N, INTERP_NONE>(t, packed, my, cbias, a, v);
+        pair_fft<N, S>(tm, t, v, a.tw, my);
+        ImageSink<N, S, SubTeam> sink{tm, a, reinterpret_cast<float*>(my + LY::OFF_SCAN)};
+        const long long ra = 2 * lp;
+        sink(t, v, ra, ra + 1 < a.m, dc);
     }
-}
-
-template <int N, int S>
-__device__ __forceinline__ void dispatch_dt_interp(const BatchDesc& d, long long u, unsigned char* smem) {
-#define OPE_B200_BATCH_INTERP(DT)                                                              \
-    switch (d.interp) {                                                                        \
-        case INTERP_NONE: batch_team_run<N, DT, INTERP_NONE, S>(d, u, smem); break;            \
-        case INTERP_LINEAR: batch_team_run<N, DT, INTERP_LINEAR, S>(d, u, smem); break;        \
-        case INTERP_CUBIC: batch_team_run<N, DT, INTERP_CUBIC, S>(d, u, smem); break;          \
-        default: batch_team_run<N, DT, INTERP_LANCZOS, S>(d, u, smem); break;                  \
-    }
-    switch (d.in_kind) {
-        case IN_U8: OPE_B200_BATCH_INTERP(IN_U8) break;
-        case IN_U16: OPE_B200_BATCH_INTERP(IN_U16) break;
-        default: OPE_B200_BATCH_INTERP(IN_F32) break;
-    }
-#undef OPE_B200_BATCH_INTERP
+    tm.sync();
+    const bool aborted = ctl->abort != 0;
+    // the region may hold another length's layout next (an aborted team's
+    // copy may still be pending: its CTA takes no further group)
+    if (t == 0 && !aborted) mbar_inval(&ctl->mbar);
+    return aborted;
 }
 
 __global__ void __launch_bounds__(BATCH_THREADS, 2)
-    batch_kernel(const BatchDesc* __restrict__ descs, int ndesc, long long total_units, unsigned long long* counter) {
+    batch_kernel(const BatchDesc* __restrict__ descs, const GroupDesc* __restrict__ groups, int ngroups,
+                 unsigned long long* counters) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(16) BatchDesc sd;
-    __shared__ long long su;
-    __shared__ int sb;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            su = (long long)atomicAdd(counter, 1ull);
-            int b = 0;
-            if (su < total_units)
-                while (b + 1 < ndesc && descs[b + 1].unit0 <= su) ++b;
-            sb = b;
-        }
+    __shared__ int enter, aborted;
+    int g0 = 0;
+    for (int g = 1; g < ngroups; ++g)
+        if (groups[g].cta_begin <= (int)blockIdx.x) g0 = g;
+    if (threadIdx.x == 0) aborted = 0;
+    for (int k = 0; k < ngroups; ++k) {
+        const int gi = (g0 + k) % ngroups;
+        const GroupDesc& g = groups[gi];
+        if (threadIdx.x == 0)
+            enter = !aborted &&
+                    *reinterpret_cast<volatile unsigned long long*>(counters + gi) < (unsigned long long)g.npairs;
         __syncthreads();
-        const long long u = su;
-        if (u >= total_units) break;
-        {
-            const int* src = reinterpret_cast<const int*>(descs + sb);
-            int* dst = reinterpret_cast<int*>(&sd);
-            for (int k = threadIdx.x; k < (int)(sizeof(BatchDesc) / 4); k += BATCH_THREADS) dst[k] = src[k];
+        if (enter) {
+            bool ab;
+            switch (g.n) {
+                case 1024:
+                    if (g.sched == 0) ab = group_run<1024, 0>(descs, &g, counters + gi, smem);
+                    else if (g.sched == 1) ab = group_run<1024, 1>(descs, &g, counters + gi, smem);
+                    else ab = group_run<1024, 2>(descs, &g, counters + gi, smem);
+                    break;
+                case 2048:
+                    if (g.sched == 0) ab = group_run<2048, 0>(descs, &g, counters + gi, smem);
+                    else if (g.sched == 1) ab = group_run<2048, 1>(descs, &g, counters + gi, smem);
+                    else ab = group_run<2048, 2>(descs, &g, counters + gi, smem);
+                    break;
+                default: ab = group_run<4096, 0>(descs, &g, counters + gi, smem); break;
+            }
+            if (ab) aborted = 1;  // benign race: every writer stores 1
         }
-        __syncthreads();
-        switch (sd.n) {
-            case 1024:
-                if (sd.sched == 0) dispatch_dt_interp<1024, 0>(sd, u, smem);
-                else if (sd.sched == 1) dispatch_dt_interp<1024, 1>(sd, u, smem);
-                else dispatch_dt_interp<1024, 2>(sd, u, smem);
-                break;
-            case 2048:
-                if (sd.sched == 0) dispatch_dt_interp<2048, 0>(sd, u, smem);
-                else if (sd.sched == 1) dispatch_dt_interp<2048, 1>(sd, u, smem);
-                else dispatch_dt_interp<2048, 2>(sd, u, smem);
-                break;
-            default: dispatch_dt_interp<4096, 0>(sd, u, smem); break;
-        }
-        __syncthreads();  // every team is done before the next unit re-lays out shared memory
+        __syncthreads();  // every team is done before shared memory takes another group's layout
     }
     if (threadIdx.x == 0) {
         __threadfence();
-        if (atomicAdd(counter + 1, 1ull) == (unsigned long long)gridDim.x - 1) {
-            counter[0] = 0;  // every CTA has left the loop: nobody reads the counter any more
-            counter[1] = 0;
+        if (atomicAdd(counters + ngroups, 1ull) == (unsigned long long)gridDim.x - 1) {
+            // every CTA has left the loop: nobody reads the counters any more
+            for (int g = 0; g <= ngroups; ++g) counters[g] = 0;
             __threadfence();
         }
     }
 }
 
-int host_team_region(int n, int kind) {
-    switch (n) {
-        case 1024: return kind == IN_U8 ? team_region<1024, IN_U8>() : kind == IN_U16 ? team_region<1024, IN_U16>()
-                                                                                       : team_region<1024, IN_F32>();
-        case 2048: return kind == IN_U8 ? team_region<2048, IN_U8>() : kind == IN_U16 ? team_region<2048, IN_U16>()
-                                                                                       : team_region<2048, IN_F32>();
-        case 4096: return kind == IN_U8 ? team_region<4096, IN_U8>() : kind == IN_U16 ? team_region<4096, IN_U16>()
-                                                                                       : team_region<4096, IN_F32>();
-        default: return 0;
-    }
+template <int N>
+constexpr int batch_region() { return BatchRegion<N>::BYTES; }
+
+int host_region(int n) {
+    return n == 1024 ? batch_region<1024>() : n == 2048 ? batch_region<2048>() : batch_region<4096>();
+}
+int host_teams(int n) { return BATCH_THREADS / (n / 16); }
+
+// Relative cost of one pair, for the CTAs' starting groups only (the groups'
+// counters balance the rest): N log N, Lanczos-8 resampling about 1.8x.
+double pair_cost(int n, int interp) {
+    int lg = 0;
+    while ((1 << lg) < n) ++lg;
+    return (double)n * lg * (interp == INTERP_LANCZOS ? 1.8 : 1.0);
 }
 
 // Radix plans per length: 1024 = 16*16*4, 4*16*16, 16*4*16; 2048 = 16*16*8,
@@ -160,15 +270,15 @@ struct ope_b200_batch {
     int device = 0;
     std::vector<ope_b200_batch_item> items;
     std::vector<BatchDesc> base;  // per item, before tuning
-    std::map<int, std::pair<int, int>> tuning;  // n -> (pairs_per_team, schedule)
+    std::map<int, std::pair<int, int>> tuning;  // n -> (pairs per grab, schedule)
     std::map<int, float> tuned_us;
     std::map<std::pair<int, int>, float2*> tw;  // (n, schedule) -> twiddles
-    BatchDesc* d_descs = nullptr;  // plain launches
-    int d_cap = 0;
-    BatchDesc* g_descs = nullptr;  // the captured graph's own copy
-    int g_cap = 0;
+    unsigned char* d_block = nullptr;  // plain launches: descriptors, then group descriptors
+    size_t d_cap = 0;
+    unsigned char* g_block = nullptr;  // the captured graph's own copy
+    size_t g_cap = 0;
     cudaEvent_t last_launch = nullptr;
-    unsigned long long* d_counter = nullptr;
+    unsigned long long* d_counter = nullptr;  // one per group, then the CTAs-done count
     int sms = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -196,55 +306,87 @@ void drop_graph(ope_b200_batch* b) {
     b->graph = nullptr;
 }
 
+constexpr int kDefaultChunk = 2;
+
 struct LaunchPlan {
-    long long units = 0;
-    int smem = 0, ndesc = 0, grid = 0;
+    const BatchDesc* descs = nullptr;
+    const GroupDesc* groups = nullptr;
+    int ngroups = 0, smem = 0, grid = 0;
 };
 
-// Descriptors of the items selected by `pick` under the current tuning,
-// uploaded to `dst` (grown as needed) with a synchronous copy, and the launch
-// configuration they need.
-int prepare(ope_b200_batch* b, const std::vector<int>& pick, BatchDesc** dst, int* cap, LaunchPlan* lp) {
+// Descriptors and group descriptors of the items selected by `pick` under the
+// current tuning, uploaded to `*dst` (grown as needed) with a synchronous
+// copy, and the launch configuration they need.
+int prepare(ope_b200_batch* b, const std::vector<int>& pick, unsigned char** dst, size_t* cap, LaunchPlan* lp) {
+    std::map<int, std::vector<int>> by_n;
+    for (int i : pick) by_n[b->base[i].n].push_back(i);
     std::vector<BatchDesc> v;
-    long long u = 0;
+    std::vector<GroupDesc> gs;
+    std::vector<double> cost;
+    double total = 0.0;
     int sm = 0;
-    for (int i : pick) {
-        BatchDesc d = b->base[i];
-        const auto tn = b->tuning.count(d.n) ? b->tuning[d.n] : std::make_pair(4, 0);
-        d.pairs_per_team = tn.first;
-        d.sched = tn.second < num_schedules(d.n) ? tn.second : 0;
-        d.a.tw = b->tw[{d.n, d.sched}];
-        const long long npairs = (d.a.m + 1) / 2;
-        const long long per_unit = (long long)d.pairs_per_team * d.teams;
-        d.unit0 = u;
-        d.units = (npairs + per_unit - 1) / per_unit;
-        u += d.units;
-        sm = std::max(sm, d.teams * d.region);
-        v.push_back(d);
+    long long team_rounds = 0;  // pairs / teams per CTA, summed over groups
+    for (const auto& kv : by_n) {
+        const int n = kv.first;
+        const auto tn = b->tuning.count(n) ? b->tuning[n] : std::make_pair(kDefaultChunk, 0);
+        GroupDesc g{};
+        g.n = n;
+        g.sched = tn.second < num_schedules(n) ? tn.second : 0;
+        g.chunk = tn.first;
+        g.first = (int)v.size();
+        g.count = (int)kv.second.size();
+        long long p = 0;
+        double c = 0.0;
+        for (int i : kv.second) {
+            BatchDesc d = b->base[i];
+            d.a.tw = b->tw[{n, g.sched}];
+            d.group = (int)gs.size();
+            d.pair0 = p;
+            d.npairs = (d.a.m + 1) / 2;
+            p += d.npairs;
+            c += (double)d.npairs * pair_cost(n, d.interp);
+            v.push_back(d);
+        }
+        g.npairs = p;
+        gs.push_back(g);
+        cost.push_back(c);
+        total += c;
+        sm = std::max(sm, host_teams(n) * host_region(n));
+        team_rounds += (p + host_teams(n) - 1) / host_teams(n);
     }
-    if ((int)v.size() > *cap) {
+    const size_t bytes = v.size() * sizeof(BatchDesc) + gs.size() * sizeof(GroupDesc);
+    if (bytes > *cap) {
         cudaFree(*dst);
         *dst = nullptr;
-        BATCH_CU(b, cudaMalloc(dst, v.size() * sizeof(BatchDesc)));
-        *cap = (int)v.size();
+        BATCH_CU(b, cudaMalloc(dst, bytes));
+        *cap = bytes;
     }
-    BATCH_CU(b, cudaMemcpy(*dst, v.data(), v.size() * sizeof(BatchDesc), cudaMemcpyHostToDevice));
     BATCH_CU(b, cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     int occ = 0;
     BATCH_CU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, BATCH_THREADS, sm));
     if (occ < 1) return bfail(b, OPE_B200_E_UNSUPPORTED, "batch kernel does not fit on an SM");
     long long grid = (long long)occ * b->sms;
-    if (grid > u) grid = u;
+    if (grid > team_rounds) grid = team_rounds;
     if (grid < 1) grid = 1;
-    lp->units = u;
+    double cum = 0.0;
+    for (size_t k = 0; k < gs.size(); ++k) {
+        gs[k].cta_begin = (int)(grid * cum / total + 0.5);
+        cum += cost[k];
+    }
+    std::vector<unsigned char> host(bytes);
+    std::memcpy(host.data(), v.data(), v.size() * sizeof(BatchDesc));
+    std::memcpy(host.data() + v.size() * sizeof(BatchDesc), gs.data(), gs.size() * sizeof(GroupDesc));
+    BATCH_CU(b, cudaMemcpy(*dst, host.data(), bytes, cudaMemcpyHostToDevice));
+    lp->descs = reinterpret_cast<const BatchDesc*>(*dst);
+    lp->groups = reinterpret_cast<const GroupDesc*>(*dst + v.size() * sizeof(BatchDesc));
+    lp->ngroups = (int)gs.size();
     lp->smem = sm;
-    lp->ndesc = (int)v.size();
     lp->grid = (int)grid;
     return OPE_B200_OK;
 }
 
-int enqueue(ope_b200_batch* b, const BatchDesc* descs, const LaunchPlan& lp, cudaStream_t s) {
-    batch_kernel<<<(unsigned)lp.grid, BATCH_THREADS, lp.smem, s>>>(descs, lp.ndesc, lp.units, b->d_counter);
+int enqueue(ope_b200_batch* b, const LaunchPlan& lp, cudaStream_t s) {
+    batch_kernel<<<(unsigned)lp.grid, BATCH_THREADS, lp.smem, s>>>(lp.descs, lp.groups, lp.ngroups, b->d_counter);
     BATCH_CU(b, cudaGetLastError());
     return OPE_B200_OK;
 }
@@ -254,9 +396,9 @@ int enqueue(ope_b200_batch* b, const BatchDesc* descs, const LaunchPlan& lp, cud
 int launch(ope_b200_batch* b, const std::vector<int>& pick, cudaStream_t s) {
     if (b->last_launch) BATCH_CU(b, cudaEventSynchronize(b->last_launch));
     LaunchPlan lp;
-    int rc = prepare(b, pick, &b->d_descs, &b->d_cap, &lp);
+    int rc = prepare(b, pick, &b->d_block, &b->d_cap, &lp);
     if (rc != OPE_B200_OK) return rc;
-    rc = enqueue(b, b->d_descs, lp, s);
+    rc = enqueue(b, lp, s);
     if (rc != OPE_B200_OK) return rc;
     BATCH_CU(b, cudaEventRecord(b->last_launch, s));
     return OPE_B200_OK;
@@ -297,15 +439,13 @@ int ope_b200_batch_create(const ope_b200_batch_item* items, int32_t count, ope_b
         d.a.out = it.d_out;
         d.a.m = it.num_ascans;
         d.a.bscans = static_cast<int>((it.num_ascans + d.a.ascans_per_bscan - 1) / d.a.ascans_per_bscan);
-        d.teams = BATCH_THREADS / (d.n / 16);
-        d.region = host_team_region(d.n, d.in_kind);
         b->items.push_back(it);
         b->base.push_back(d);
     }
     cudaError_t e = cudaSetDevice(b->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, 2 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(b->d_counter, 0, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, (BATCH_MAX_GROUPS + 1) * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(b->d_counter, 0, (BATCH_MAX_GROUPS + 1) * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->last_launch, cudaEventDisableTiming);
     for (const BatchDesc& d : b->base)
@@ -332,8 +472,8 @@ void ope_b200_batch_destroy(ope_b200_batch* b) {
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     if (b->last_launch) cudaEventDestroy(b->last_launch);
     for (auto& kv : b->tw) cudaFree(kv.second);
-    cudaFree(b->d_descs);
-    cudaFree(b->g_descs);
+    cudaFree(b->d_block);
+    cudaFree(b->g_block);
     cudaFree(b->d_counter);
     delete b;
 }
@@ -355,7 +495,7 @@ int ope_b200_batch_set_tuning(ope_b200_batch* b, int32_t n, int32_t pairs_per_te
 int ope_b200_batch_get_tuning(ope_b200_batch* b, int32_t n, int32_t* pairs_per_team, int32_t* radix_schedule,
                               float* best_us) {
     if (!b) return OPE_B200_E_INVALID;
-    const auto tn = b->tuning.count(n) ? b->tuning[n] : std::make_pair(4, 0);
+    const auto tn = b->tuning.count(n) ? b->tuning[n] : std::make_pair(kDefaultChunk, 0);
     if (pairs_per_team) *pairs_per_team = tn.first;
     if (radix_schedule) *radix_schedule = tn.second;
     if (best_us) *best_us = b->tuned_us.count(n) ? b->tuned_us[n] : -1.0f;
@@ -376,10 +516,10 @@ int ope_b200_batch_run_graph(ope_b200_batch* b, void* stream) {
         // only the kernel launch is captured
         BATCH_CU(b, cudaDeviceSynchronize());
         LaunchPlan lp;
-        int rc = prepare(b, all_items(b), &b->g_descs, &b->g_cap, &lp);
+        int rc = prepare(b, all_items(b), &b->g_block, &b->g_cap, &lp);
         if (rc != OPE_B200_OK) return rc;
         BATCH_CU(b, cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-        rc = enqueue(b, b->g_descs, lp, b->cap_stream);
+        rc = enqueue(b, lp, b->cap_stream);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
         if (rc != OPE_B200_OK) {
@@ -404,12 +544,12 @@ int ope_b200_batch_autotune(ope_b200_batch* b, int32_t reps) {
     BATCH_CU(b, cudaEventCreate(&e1));
     std::map<int, std::vector<int>> by_len;
     for (size_t i = 0; i < b->base.size(); ++i) by_len[b->base[i].n].push_back((int)i);
-    static const int kPairs[] = {1, 2, 4, 8, 16, 32};
+    static const int kPairs[] = {1, 2, 4, 8};
     int rc = OPE_B200_OK;
     for (auto& kv : by_len) {
         const int n = kv.first;
         float best = 1e30f;
-        std::pair<int, int> best_cfg{4, 0};
+        std::pair<int, int> best_cfg{kDefaultChunk, 0};
         for (int sched = 0; sched < num_schedules(n) && rc == OPE_B200_OK; ++sched)
             for (int pp : kPairs) {
                 b->tuning[n] = {pp, sched};

@@ -223,6 +223,110 @@ __device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, con
         }
 }
 
+// One pair's staged rows -> the team's spectrum: the optional bitshift, then
+// the packed integer spectrum (8/16-bit samples without rolling-average DC
+// removal), rolling-average DC removal (exact sums or the reference's order),
+// the exact DC split, or the plain unpack. `smem` is the team's region laid
+// out as Layout<N, DT>; returns whether the packed spectrum was written, with
+// the split-off DC level in `dc` and the packed taps' bias in `cbias`.
+// Ends with the stage consumed but WITHOUT a closing barrier.
+template <int N, int DT, class Team>
+__device__ __forceinline__ bool pair_unpack(const Team& tm, int t, const ChainArgs& a, unsigned char* smem,
+                                            float2& dc, float2& cbias) {
+    using LY = Layout<N, DT>;
+    using sum_t = typename InTraits<DT>::sum_t;
+    constexpr int T = Plan<N>::T;
+    float2* spec = reinterpret_cast<float2*>(smem + LY::OFF_SPEC);
+    sum_t* pfx = reinterpret_cast<sum_t*>(smem + LY::OFF_PFX);
+    sum_t* scan = reinterpret_cast<sum_t*>(smem + LY::OFF_SCAN);
+    unsigned char* stages = smem + LY::OFF_STAGE;
+    const unsigned char* stage = stages;
+    if constexpr (DT == IN_U8 || DT == IN_U16) {
+        if (a.bitshift) {
+            phase_bitshift<N, DT>(t, stages);
+            tm.sync();
+        }
+    }
+    dc = make_float2(0.0f, 0.0f);
+    // 8/16-bit samples without rolling-average DC removal: packed integer
+    // spectrum (bit-identical taps, half the shared-memory bytes)
+    constexpr bool PACKABLE = (DT == IN_U8 || DT == IN_U16);
+    const bool packed = PACKABLE && a.dc_window == 0;
+    cbias = dup2(8388608.0f);
+    if (packed) {
+        uint32_t words[16];
+        int sa, sb;
+        phase_split_load_packed<N, DT>(t, stage, words, &sa, &sb);
+        if (a.dc_resp) {
+            team_sum2<T, int>(tm, sa, sb, reinterpret_cast<int*>(scan));
+            dc = make_float2(split_level((double)sa, N, true), split_level((double)sb, N, true));
+            cbias = add2(cbias, dc);  // 2^23 + c, exact for c < 2^23
+        }
+        phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
+    } else if (a.dc_window > 0 && a.dc_ref_order) {
+        phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
+        tm.sync();
+        phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);
+    } else if (a.dc_window > 0) {
+        sum_t ta, tb;
+        phase_dc_local<N, DT>(t, stage, &ta, &tb);
+        team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan);
+        phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
+        tm.sync();
+        phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
+    } else if (a.dc_resp) {
+        using SS = typename SplitSum<DT>::type;
+        float2 vals[16];
+        SS sa, sb;
+        phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
+        team_sum2<T, SS>(tm, sa, sb, reinterpret_cast<SS*>(scan));
+        dc = make_float2(split_level((double)sa, N, DT != IN_F32), split_level((double)sb, N, DT != IN_F32));
+        phase_split_store<N>(t, vals, dc, spec);
+    } else {
+        phase_unpack<N, DT>(t, stage, spec);
+    }
+    return packed;
+}
+
+// k-linearisation, window and phase of one pair from the team's spectrum
+// (the packed integer one when `packed`) into the pass-0 inputs v.
+template <int N, int INTERP>
+__device__ __forceinline__ void pair_prestage(int t, bool packed, const unsigned char* smem, float2 cbias,
+                                              const ChainArgs& a, cp* v) {
+    const float2* spec = reinterpret_cast<const float2*>(smem + Layout<N, IN_U16>::OFF_SPEC);
+    if (packed) phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v);
+    else phase_prestage<N, INTERP>(t, spec, a, v);
+}
+
+// The Stockham passes of radix schedule S up to the last one, whose bins stay
+// in v (bin layout of LastInfo<N, S>). The exchange buffer aliases the
+// spectrum: the first barrier orders every thread's spectrum reads before it.
+template <int N, int S, class Team>
+__device__ __forceinline__ void pair_fft(const Team& tm, int t, cp* v, const float2* tw, unsigned char* smem) {
+    constexpr int NPASS = Plan<N>::NPASS;
+    float4* exch = reinterpret_cast<float4*>(smem + Layout<N, IN_U16>::OFF_EXCH);
+    fft_twiddle_dft<N, 0, false, S>(t, v, tw);
+    tm.sync();  // spec aliases the exchange buffer
+    fft_store<N, 0, S>(t, v, exch);
+    tm.sync();
+    if constexpr (NPASS > 2) {
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, 1, false, S>(t, v, tw);
+        tm.sync();
+        fft_store<N, 1, S>(t, v, exch);
+        tm.sync();
+    }
+    if constexpr (NPASS > 3) {
+        fft_load<N>(t, exch, v);
+        fft_twiddle_dft<N, 2, false, S>(t, v, tw);
+        tm.sync();
+        fft_store<N, 2, S>(t, v, exch);
+        tm.sync();
+    }
+    fft_load<N>(t, exch, v);
+    fft_twiddle_dft<N, NPASS - 1, false, S>(t, v, tw);
+}
+
 // Runs the chain up to the last FFT pass for the pairs p = p0, p0 + step, ...
 // (< p_end) whose rows are row0 + 2p and row0 + 2p + 1 (the second one only if
 // < row_end), and hands each pair's bins to `sink(t, v, row_a, has_b)`.
@@ -237,17 +341,9 @@ template <int N, int DT, int INTERP, int S, class Team, class Sink>
 __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, long long row0, long long row_end,
                                           long long p0, long long p_end, long long step, unsigned char* smem,
                                           Sink& sink) {
-    using PL = Plan<N>;
     using LY = Layout<N, DT>;
-    using sum_t = typename InTraits<DT>::sum_t;
     using raw_t = typename InTraits<DT>::raw_t;
-    constexpr int T = PL::T;
-    constexpr int NPASS = PL::NPASS;
 
-    float2* spec = reinterpret_cast<float2*>(smem + LY::OFF_SPEC);
-    float4* exch = reinterpret_cast<float4*>(smem + LY::OFF_EXCH);
-    sum_t* pfx = reinterpret_cast<sum_t*>(smem + LY::OFF_PFX);
-    sum_t* scan = reinterpret_cast<sum_t*>(smem + LY::OFF_SCAN);
     unsigned char* stages = smem + LY::OFF_STAGE;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + LY::OFF_MBAR);
     int* abort_flag = reinterpret_cast<int*>(smem + LY::OFF_MBAR + 16);
@@ -298,83 +394,16 @@ __device__ __forceinline__ void run_pairs(const Team& tm, const ChainArgs& a, lo
             }
             return;
         }
-        const unsigned char* stage = stages;
-        if constexpr (DT == IN_U8 || DT == IN_U16) {
-            if (a.bitshift) {
-                phase_bitshift<N, DT>(t, stages);
-                tm.sync();
-            }
-        }
-
-        // ---- unpack (+ DC removal or exact DC split) ----
-        float2 dc = make_float2(0.0f, 0.0f);
-        // 8/16-bit samples without rolling-average DC removal: packed integer
-        // spectrum (bit-identical taps, half the shared-memory bytes)
-        constexpr bool PACKABLE = (DT == IN_U8 || DT == IN_U16);
-        const bool packed = PACKABLE && a.dc_window == 0;
-        float2 cbias = dup2(8388608.0f);
-        if (packed) {
-            uint32_t words[16];
-            int sa, sb;
-            phase_split_load_packed<N, DT>(t, stage, words, &sa, &sb);
-            if (a.dc_resp) {
-                team_sum2<T, int>(tm, sa, sb, reinterpret_cast<int*>(scan));
-                dc = make_float2(split_level((double)sa, N, true), split_level((double)sb, N, true));
-                cbias = add2(cbias, dc);  // 2^23 + c, exact for c < 2^23
-            }
-            phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
-        } else if (a.dc_window > 0 && a.dc_ref_order) {
-            phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
-            tm.sync();
-            phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);
-        } else if (a.dc_window > 0) {
-            sum_t ta, tb;
-            phase_dc_local<N, DT>(t, stage, &ta, &tb);
-            team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan);
-            phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
-            tm.sync();
-            phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
-        } else if (a.dc_resp) {
-            using SS = typename SplitSum<DT>::type;
-            float2 vals[16];
-            SS sa, sb;
-            phase_split_load<N, DT>(t, stage, vals, &sa, &sb);
-            team_sum2<T, SS>(tm, sa, sb, reinterpret_cast<SS*>(scan));
-            dc = make_float2(split_level((double)sa, N, DT != IN_F32), split_level((double)sb, N, DT != IN_F32));
-            phase_split_store<N>(t, vals, dc, spec);
-        } else {
-            phase_unpack<N, DT>(t, stage, spec);
-        }
+        float2 dc, cbias;
+        const bool packed = pair_unpack<N, DT>(tm, t, a, smem, dc, cbias);
         tm.sync();
         if (t == 0) {  // every thread is done with the stage
             issued = nxt < p_end;
             if (issued) issue(nxt);
         }
-
-        // ---- k-linearisation, window, phase; pass 0 ----
         cp v[16];
-        if (packed) phase_prestage_packed<N, INTERP>(t, reinterpret_cast<const uint32_t*>(spec), cbias, a, v);
-        else phase_prestage<N, INTERP>(t, spec, a, v);
-        fft_twiddle_dft<N, 0, false, S>(t, v, a.tw);
-        tm.sync();  // spec aliases the exchange buffer
-        fft_store<N, 0, S>(t, v, exch);
-        tm.sync();
-        if constexpr (NPASS > 2) {
-            fft_load<N>(t, exch, v);
-            fft_twiddle_dft<N, 1, false, S>(t, v, a.tw);
-            tm.sync();
-            fft_store<N, 1, S>(t, v, exch);
-            tm.sync();
-        }
-        if constexpr (NPASS > 3) {
-            fft_load<N>(t, exch, v);
-            fft_twiddle_dft<N, 2, false, S>(t, v, a.tw);
-            tm.sync();
-            fft_store<N, 2, S>(t, v, exch);
-            tm.sync();
-        }
-        fft_load<N>(t, exch, v);
-        fft_twiddle_dft<N, NPASS - 1, false, S>(t, v, a.tw);
+        pair_prestage<N, INTERP>(t, packed, smem, cbias, a, v);
+        pair_fft<N, S>(tm, t, v, a.tw, smem);
         const long long ra = row0 + 2 * item;
         sink(t, v, ra, ra + 1 < row_end, dc);
         // the next item's writes to spec/exch come after the barrier at the top
