@@ -8,20 +8,21 @@
 // described by an ope_b200_ctx (its ProcessorConfiguration and curves), so
 // every buffer gets exactly the chain a single-buffer call would run.
 //
-// Work decomposition. The buffers are grouped by length N; a group's A-scan
-// pairs are numbered consecutively over its buffers. A CTA has 256 threads
-// and, while it works on a group, runs 4096/N teams of N/16 threads (each
-// with its own named barrier and shared-memory region laid out for the
-// widest input type), every team running the single-buffer kernel's
-// pair-of-A-scans pipeline (pair_unpack, pair_prestage, pair_fft, the image
-// epilogue) with the input type and resampling mode of each pair's buffer
-// chosen at run time. Teams take pairs from the group's counter in grabs of
-// `chunk` pairs and stage the next pair (of any buffer of the group) while
-// computing the current one, so the copy/compute pipeline runs unbroken
-// across grabs and buffers. Each CTA starts on the group whose CTA range
-// (proportional to the group's estimated work) holds it and then visits the
-// other groups in turn, entering only those with pairs left; the last CTA to
-// finish resets the counters, so a captured graph replays without a memset.
+// Work decomposition. The buffers are grouped by length N and stage width
+// (8/16-bit samples apart from float ones); a group's A-scan pairs are
+// numbered consecutively over its buffers. A CTA has 256 threads and, while
+// it works on a group, runs 4096/N teams of N/16 threads (each with its own
+// named barrier and shared-memory region), every team running the
+// single-buffer kernel's pair-of-A-scans pipeline (pair_unpack,
+// pair_prestage, pair_fft, the image epilogue) with the input type and
+// resampling mode of each pair's buffer chosen at run time. Teams take pairs
+// from the group's counter in grabs of `chunk` pairs and stage the next pair
+// (of any buffer of the group) while computing the current one, so the
+// copy/compute pipeline runs unbroken across grabs and buffers. Each CTA
+// starts on the group whose CTA range (proportional to the group's estimated
+// work) holds it and then visits the other groups in turn, entering only
+// those with pairs left; the last CTA to finish resets the counters, so a
+// captured graph replays without a memset.
 // The autotuner picks the grab size and the FFT radix schedule per length by
 // timing this batch's own buffers of that length.
 #include <cuda_runtime.h>
@@ -43,7 +44,7 @@ int ctx_batch_args(ope_b200_ctx* c, ChainArgs* a, int* n, int* in_kind, int* int
 const char* ctx_error(const ope_b200_ctx* c);
 
 constexpr int BATCH_THREADS = 256;
-constexpr int BATCH_MAX_GROUPS = 3;  // one per supported length
+constexpr int BATCH_MAX_GROUPS = 6;  // one per supported length and stage width
 
 struct BatchDesc {
     ChainArgs a;
@@ -59,24 +60,31 @@ struct GroupDesc {
     long long npairs;   // pairs of all the group's buffers
     int chunk;          // pairs per grab
     int cta_begin;      // first CTA that starts on this group
+    int wide;           // 1: float samples (4-byte stage), 0: 8/16-bit samples (2-byte stage)
+    int pad;
 };
 
-// One team's region: Layout<N, IN_F32> (the widest stage); the spectrum,
-// prefix, scan and exchange offsets are the same for 8-, 16-bit and float
-// samples, so pair_unpack<N, DT> of any of them works in it.
-template <int N>
+// One team's region: the spectrum, prefix, scan and exchange areas and the
+// stage at the offsets of Layout<N, DT> (the same for 8-, 16-bit and float
+// samples, so pair_unpack<N, DT> of any of them works in it), the stage sized
+// for W-byte samples (W = 2 for a group of 8/16-bit buffers, 4 for float
+// ones), then the control words. Groups are split by stage width so that a
+// group of 8/16-bit buffers keeps the single-buffer kernel's shared-memory
+// footprint, which leaves the L1 share of the SM's memory to the table reads.
+template <int N, int W>
 struct BatchRegion {
-    using LY = Layout<N, IN_F32>;
-    static_assert(Layout<N, IN_U8>::OFF_STAGE == LY::OFF_STAGE && Layout<N, IN_U16>::OFF_STAGE == LY::OFF_STAGE &&
-                      Layout<N, IN_U8>::OFF_SCAN == LY::OFF_SCAN && Layout<N, IN_U16>::OFF_SCAN == LY::OFF_SCAN &&
-                      Layout<N, IN_U8>::OFF_PFX == LY::OFF_PFX && Layout<N, IN_U16>::OFF_PFX == LY::OFF_PFX,
+    using LY = Layout<N, IN_U16>;
+    static_assert(Layout<N, IN_U8>::OFF_STAGE == LY::OFF_STAGE && Layout<N, IN_F32>::OFF_STAGE == LY::OFF_STAGE &&
+                      Layout<N, IN_U8>::OFF_SCAN == LY::OFF_SCAN && Layout<N, IN_F32>::OFF_SCAN == LY::OFF_SCAN &&
+                      Layout<N, IN_U8>::OFF_PFX == LY::OFF_PFX && Layout<N, IN_F32>::OFF_PFX == LY::OFF_PFX,
                   "batched teams share one layout for every input type");
-    static constexpr int BYTES = ((LY::TOTAL + 127) / 128) * 128;
     static constexpr int TEAMS = BATCH_THREADS / (N / 16);
+    static constexpr int CTL = LY::OFF_STAGE + 2 * N * W;  // control words after the stage
+    static constexpr int BYTES = (CTL + 64 + 127) / 128 * 128;
 };
 
-// Team control words after a team's mbarrier (Layout::OFF_MBAR, 64 bytes):
-// the abort flag, the staged pair (descriptor, pair within its buffer) and
+// A team's control words (64 bytes at BatchRegion::CTL): its mbarrier, the
+// abort flag, the staged pair (descriptor, pair within its buffer) and
 // thread 0's grab [lo, hi) and descriptor cursor.
 struct TeamCtl {
     uint64_t mbar;
@@ -88,7 +96,7 @@ struct TeamCtl {
     int cursor;
     int pad2;
 };
-static_assert(sizeof(TeamCtl) <= 64, "team control words fit the mbarrier slot");
+static_assert(sizeof(TeamCtl) <= 64, "team control words fit their 64-byte slot");
 
 __device__ __forceinline__ uint32_t in_bytes(int kind) { return kind == IN_U8 ? 1u : kind == IN_U16 ? 2u : 4u; }
 
@@ -97,11 +105,12 @@ __device__ __forceinline__ uint32_t in_bytes(int kind) { return kind == IN_U8 ? 
 // in the control words and issues the copy of its rows into the stage; or
 // publishes "none". A team's pairs only increase, so the descriptor cursor
 // only moves forward.
-template <int N>
-__device__ __noinline__ void team_stage_next(const BatchDesc* __restrict__ descs, const GroupDesc* g,
-                                             unsigned long long* counter, unsigned char* my) {
-    using LY = typename BatchRegion<N>::LY;
-    TeamCtl* c = reinterpret_cast<TeamCtl*>(my + LY::OFF_MBAR);
+template <int N, int W>
+__device__ __forceinline__ void team_stage_next(const BatchDesc* __restrict__ descs, const GroupDesc* g,
+                                                unsigned long long* counter, unsigned char* my) {
+    using R = BatchRegion<N, W>;
+    using LY = typename R::LY;
+    TeamCtl* c = reinterpret_cast<TeamCtl*>(my + R::CTL);
     if (c->grab_lo >= c->grab_hi) {
         const long long s = (long long)atomicAdd(counter, (unsigned long long)g->chunk);
         if (s >= g->npairs) {
@@ -132,16 +141,16 @@ __device__ __noinline__ void team_stage_next(const BatchDesc* __restrict__ descs
 // time through the pipeline, the next pair's copy issued as soon as the
 // current pair's rows are unpacked. Returns whether a bounded wait ran out
 // (the team stops; the status word says so).
-template <int N, int S>
+template <int N, int S, int W>
 __device__ __forceinline__ bool group_run(const BatchDesc* __restrict__ descs, const GroupDesc* g,
                                           unsigned long long* counter, unsigned char* smem) {
-    using R = BatchRegion<N>;
+    using R = BatchRegion<N, W>;
     using LY = typename R::LY;
     constexpr int T = N / 16;
     const int team = threadIdx.x / T;
     const SubTeam tm{team * T, 1 + team, T};
     unsigned char* my = smem + team * R::BYTES;
-    TeamCtl* ctl = reinterpret_cast<TeamCtl*>(my + LY::OFF_MBAR);
+    TeamCtl* ctl = reinterpret_cast<TeamCtl*>(my + R::CTL);
     const int t = tm.tid();
     if (t == 0) {
         mbar_init(&ctl->mbar, 1);
@@ -149,7 +158,7 @@ __device__ __forceinline__ bool group_run(const BatchDesc* __restrict__ descs, c
         ctl->abort = 0;
         ctl->grab_lo = ctl->grab_hi = 0;
         ctl->cursor = g->first;
-        team_stage_next<N>(descs, g, counter, my);
+        team_stage_next<N, W>(descs, g, counter, my);
     }
     tm.sync();
     for (int it = 0;; ++it) {
@@ -172,12 +181,16 @@ __device__ __forceinline__ bool group_run(const BatchDesc* __restrict__ descs, c
         float2 dc, cbias;
         bool packed;
         const int kind = descs[cd].in_kind;
-        if (kind == IN_U8) packed = pair_unpack<N, IN_U8>(tm, t, a, my, dc, cbias);
-        else if (kind == IN_U16) packed = pair_unpack<N, IN_U16>(tm, t, a, my, dc, cbias);
-        else packed = pair_unpack<N, IN_F32>(tm, t, a, my, dc, cbias);
+        if constexpr (W == 4) {
+            (void)kind;
+            packed = pair_unpack<N, IN_F32>(tm, t, a, my, dc, cbias);
+        } else {
+            if (kind == IN_U8) packed = pair_unpack<N, IN_U8>(tm, t, a, my, dc, cbias);
+            else packed = pair_unpack<N, IN_U16>(tm, t, a, my, dc, cbias);
+        }
         tm.sync();
         // every thread is done with the stage and has read next_*
-        if (t == 0) team_stage_next<N>(descs, g, counter, my);
+        if (t == 0) team_stage_next<N, W>(descs, g, counter, my);
         cp v[16];
         const int interp = descs[cd].interp;
         if (interp == INTERP_CUBIC) pair_prestage<N, INTERP_CUBIC>(t, packed, my, cbias, a, v);
@@ -195,6 +208,22 @@ __device__ __forceinline__ bool group_run(const BatchDesc* __restrict__ descs, c
     // copy may still be pending: its CTA takes no further group)
     if (t == 0 && !aborted) mbar_inval(&ctl->mbar);
     return aborted;
+}
+
+template <int W>
+__device__ __forceinline__ bool group_dispatch(const BatchDesc* __restrict__ descs, const GroupDesc& g,
+                                               unsigned long long* counter, unsigned char* smem) {
+    switch (g.n) {
+        case 1024:
+            if (g.sched == 0) return group_run<1024, 0, W>(descs, &g, counter, smem);
+            if (g.sched == 1) return group_run<1024, 1, W>(descs, &g, counter, smem);
+            return group_run<1024, 2, W>(descs, &g, counter, smem);
+        case 2048:
+            if (g.sched == 0) return group_run<2048, 0, W>(descs, &g, counter, smem);
+            if (g.sched == 1) return group_run<2048, 1, W>(descs, &g, counter, smem);
+            return group_run<2048, 2, W>(descs, &g, counter, smem);
+        default: return group_run<4096, 0, W>(descs, &g, counter, smem);
+    }
 }
 
 __global__ void __launch_bounds__(BATCH_THREADS, 2)
@@ -215,19 +244,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2)
         __syncthreads();
         if (enter) {
             bool ab;
-            switch (g.n) {
-                case 1024:
-                    if (g.sched == 0) ab = group_run<1024, 0>(descs, &g, counters + gi, smem);
-                    else if (g.sched == 1) ab = group_run<1024, 1>(descs, &g, counters + gi, smem);
-                    else ab = group_run<1024, 2>(descs, &g, counters + gi, smem);
-                    break;
-                case 2048:
-                    if (g.sched == 0) ab = group_run<2048, 0>(descs, &g, counters + gi, smem);
-                    else if (g.sched == 1) ab = group_run<2048, 1>(descs, &g, counters + gi, smem);
-                    else ab = group_run<2048, 2>(descs, &g, counters + gi, smem);
-                    break;
-                default: ab = group_run<4096, 0>(descs, &g, counters + gi, smem); break;
-            }
+            if (g.wide) ab = group_dispatch<4>(descs, g, counters + gi, smem);
+            else ab = group_dispatch<2>(descs, g, counters + gi, smem);
             if (ab) aborted = 1;  // benign race: every writer stores 1
         }
         __syncthreads();  // every team is done before shared memory takes another group's layout
@@ -242,12 +260,11 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2)
     }
 }
 
-template <int N>
-constexpr int batch_region() { return BatchRegion<N>::BYTES; }
-
-int host_region(int n) {
-    return n == 1024 ? batch_region<1024>() : n == 2048 ? batch_region<2048>() : batch_region<4096>();
+template <int W>
+int host_region_w(int n) {
+    return n == 1024 ? BatchRegion<1024, W>::BYTES : n == 2048 ? BatchRegion<2048, W>::BYTES : BatchRegion<4096, W>::BYTES;
 }
+int host_region(int n, bool wide) { return wide ? host_region_w<4>(n) : host_region_w<2>(n); }
 int host_teams(int n) { return BATCH_THREADS / (n / 16); }
 
 // Relative cost of one pair, for the CTAs' starting groups only (the groups'
@@ -318,8 +335,9 @@ struct LaunchPlan {
 // current tuning, uploaded to `*dst` (grown as needed) with a synchronous
 // copy, and the launch configuration they need.
 int prepare(ope_b200_batch* b, const std::vector<int>& pick, unsigned char** dst, size_t* cap, LaunchPlan* lp) {
-    std::map<int, std::vector<int>> by_n;
-    for (int i : pick) by_n[b->base[i].n].push_back(i);
+    // groups: one per (length, stage width), float buffers apart from 8/16-bit ones
+    std::map<std::pair<int, int>, std::vector<int>> by_n;
+    for (int i : pick) by_n[{b->base[i].n, b->base[i].in_kind == IN_F32 ? 1 : 0}].push_back(i);
     std::vector<BatchDesc> v;
     std::vector<GroupDesc> gs;
     std::vector<double> cost;
@@ -327,10 +345,11 @@ int prepare(ope_b200_batch* b, const std::vector<int>& pick, unsigned char** dst
     int sm = 0;
     long long team_rounds = 0;  // pairs / teams per CTA, summed over groups
     for (const auto& kv : by_n) {
-        const int n = kv.first;
+        const int n = kv.first.first;
         const auto tn = b->tuning.count(n) ? b->tuning[n] : std::make_pair(kDefaultChunk, 0);
         GroupDesc g{};
         g.n = n;
+        g.wide = kv.first.second;
         g.sched = tn.second < num_schedules(n) ? tn.second : 0;
         g.chunk = tn.first;
         g.first = (int)v.size();
@@ -351,7 +370,7 @@ int prepare(ope_b200_batch* b, const std::vector<int>& pick, unsigned char** dst
         gs.push_back(g);
         cost.push_back(c);
         total += c;
-        sm = std::max(sm, host_teams(n) * host_region(n));
+        sm = std::max(sm, host_teams(n) * host_region(n, g.wide != 0));
         team_rounds += (p + host_teams(n) - 1) / host_teams(n);
     }
     const size_t bytes = v.size() * sizeof(BatchDesc) + gs.size() * sizeof(GroupDesc);
