@@ -565,16 +565,28 @@ OPE_HD float sample_as_float(const unsigned char* stage, int n, int row, int i) 
     return (float)x;
 }
 
+// The samples are read in chunks of 32 into registers before the chunk's 32
+// dependent additions: the prefix stores go to shared memory too, so a load
+// after a store could not be issued ahead of it, and each step would wait
+// out a shared-memory round trip instead of one addition.
 template <int N, int DT>
 OPE_HD void phase_dc_ref_scan(int t, const unsigned char* stage, float* pf) {
     if (t > 1) return;
+    constexpr int C = 32;
+    static_assert(N % C == 0, "whole chunks");
     float s = 0.0f;
     pf[pfx_idx(t)] = 0.0f;
-#pragma unroll 8
-    for (int i = 0; i < N; ++i) {
-        s = fadd_rn(s, sample_as_float<DT>(stage, N, t, i));
-        OPE_SMEM_CHECK(pfx_idx(2 * (i + 1) + t) < pfx_idx(2 * (N + 1)));
-        pf[pfx_idx(2 * (i + 1) + t)] = s;
+#pragma unroll 1
+    for (int i0 = 0; i0 < N; i0 += C) {
+        float xs[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) xs[k] = sample_as_float<DT>(stage, N, t, i0 + k);
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            s = fadd_rn(s, xs[k]);
+            OPE_SMEM_CHECK(pfx_idx(2 * (i0 + k + 1) + t) < pfx_idx(2 * (N + 1)));
+            pf[pfx_idx(2 * (i0 + k + 1) + t)] = s;
+        }
     }
 }
 
