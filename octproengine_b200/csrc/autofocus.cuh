@@ -140,14 +140,15 @@ template <int N, int DT>
 struct AfLayout {
     using raw_t = typename InTraits<DT>::raw_t;
     static constexpr int ROW_BYTES = N * (int)sizeof(raw_t);
+    // the spectrum overlays the raw rows: the unpack holds a pair's samples in
+    // registers across the team sum before it writes the spectrum
     static constexpr int OFF_STAGE = 0;
-    static constexpr int OFF_SPEC = ((2 * ROW_BYTES + 127) / 128) * 128;
-    static constexpr int OFF_EXCH = ((OFF_SPEC + (N + 2 * SPEC_PAD) * 8 + 127) / 128) * 128;
+    static constexpr int OFF_SPEC = 0;
+    static constexpr int SPEC_OR_STAGE = (N + 2 * SPEC_PAD) * 8 > 2 * ROW_BYTES ? (N + 2 * SPEC_PAD) * 8 : 2 * ROW_BYTES;
+    static constexpr int OFF_EXCH = ((SPEC_OR_STAGE + 127) / 128) * 128;
     static constexpr int OFF_SCAN = OFF_EXCH + Plan<N>::EXCH_ELEMS * 16;
-    // the resampled samples y of the pair, kept for the dispersion-only adjoint
-    static constexpr int OFF_Y = OFF_SCAN + 1024;
-    static constexpr int TOTAL = OFF_Y + N * 8;
-    static_assert(OFF_SPEC % 128 == 0 && OFF_EXCH % 128 == 0 && OFF_SCAN % 16 == 0 && OFF_Y % 16 == 0,
+    static constexpr int TOTAL = OFF_SCAN + 1024;
+    static_assert(OFF_SPEC % 128 == 0 && OFF_EXCH % 128 == 0 && OFF_SCAN % 16 == 0,
                   "shared-memory regions must stay aligned for their widest accesses");
 };
 
@@ -244,8 +245,17 @@ __device__ __forceinline__ void af_cta_sum8(const float* v, double* scratch, dou
     }
 }
 
+// CTAs per SM the adjoint's registers are capped for: 4 at N = 2048 (128
+// registers; its shared memory also allows 4, so the 512 pairs of a
+// 1024-A-scan B-scan take one round), 8 at N = 1024, 1 at N = 4096 (whose
+// shared memory allows only one).
+template <int N>
+struct AfBwdOcc {
+    static constexpr int MIN_BLOCKS = N <= 1024 ? 8 : N == 2048 ? 4 : 1;
+};
+
 template <int N, int DT, int INTERP>
-__global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) {
+__global__ void __launch_bounds__(N / 16, AfBwdOcc<N>::MIN_BLOCKS) af_backward_kernel(const AfArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     using PL = Plan<N>;
     using LY = AfLayout<N, DT>;
@@ -257,7 +267,6 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
     float2* spec = reinterpret_cast<float2*>(smem + LY::OFF_SPEC);
     float4* exch = reinterpret_cast<float4*>(smem + LY::OFF_EXCH);
     double* scan = reinterpret_cast<double*>(smem + LY::OFF_SCAN);
-    float2* ybuf = reinterpret_cast<float2*>(smem + LY::OFF_Y);
     const int t = threadIdx.x;
     const ChainArgs& c = a.c;
     const long long m = c.m;
@@ -312,12 +321,11 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
         // ---- recompute the forward up to X ----
         cp v[16];
         if (a.disp_only) {
-            // y kept in shared memory: the dispersion adjoint needs y, not dy/dr
+            // the dispersion adjoint needs y, not dy/dr (recomputed below from the spectrum)
 #pragma unroll
             for (int s2 = 0; s2 < 16; ++s2) {
                 const int j = t + s2 * T;
                 const float2 y = af_interp_value<N, INTERP>(spec, a, j);
-                ybuf[j] = y;
                 const float2 q = __ldg(c.wph + j);
                 v[s2] = cpmake(mul2(y, dup2(q.x)), mul2(y, dup2(q.y)));
             }
@@ -407,7 +415,7 @@ __global__ void __launch_bounds__(N / 16, 2) af_backward_kernel(const AfArgs a) 
                 float2 y, dy;
                 float gr = 0.0f;
                 if (a.disp_only) {
-                    y = ybuf[j];
+                    y = af_interp_value<N, INTERP>(spec, a, j);
                 } else {
                     af_interp_deriv<N, INTERP>(spec, a, j, y, dy);
                     const float2 gy2 = mul2(hre, dy);
