@@ -734,6 +734,26 @@ def run_ours(args):
     variants["lanczos8"] = {"value": M / (lms / 1e3), "unit": UNIT, "ms_per_step": lms,
                             "hbm_frac": bytes_launch / (lms / 1e3) / 1e9 / peak}
     ctx_l.close()
+    # rolling-average DC removal (window 64) on the same buffer: exact window
+    # sums; the reference's float prefix order on these full-range 16-bit
+    # samples (row totals above 2^24: the serial prefix); and the reference
+    # order on 12-bit samples (the same buffer through DataParameters::bitshift:
+    # row totals below 2^24, so the exact prefix equals the float one)
+    for name, kw in (("rolling_dc_exact_sums", {}), ("rolling_dc_reference_order", {"dc_reference_order": True}),
+                     ("rolling_dc_reference_order_12bit", {"dc_reference_order": True, "bitshift": True})):
+        ctx_d = open_context(spec.with_(dc_removal=True, dc_window=64, **kw))
+        ctx_d.set_fpn_profile(ctx.fpn_profile())
+        for _ in range(2):
+            ctx_d.process_device(x.data_ptr(), out.data_ptr(), sp)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(reps):
+            ctx_d.process_device(x.data_ptr(), out.data_ptr(), sp)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        dms = e0.elapsed_time(e1) / reps
+        variants[name] = {"value": M / (dms / 1e3), "unit": UNIT, "ms_per_step": dms}
+        ctx_d.close()
     e0.record(stream)
     for _ in range(reps):
         ctx.request_fpn_determination()

@@ -87,9 +87,11 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Exclusive team scan of two values per thread (T threads, T % 32 == 0).
+// Exclusive team scan of two values per thread (T threads, T % 32 == 0);
+// the team totals too when tot_a / tot_b are given.
 template <int T, typename S, class Team>
-__device__ __forceinline__ void team_exclusive_scan2(const Team& tm, S& a, S& b, S* scratch) {
+__device__ __forceinline__ void team_exclusive_scan2(const Team& tm, S& a, S& b, S* scratch, S* tot_a = nullptr,
+                                                     S* tot_b = nullptr) {
     const int lane = tm.tid() & 31, warp = tm.tid() >> 5;
     S ia = a, ib = b;
 #pragma unroll
@@ -110,6 +112,15 @@ __device__ __forceinline__ void team_exclusive_scan2(const Team& tm, S& a, S& b,
     for (int w = 0; w < warp; ++w) {
         pa += scratch[2 * w];
         pb += scratch[2 * w + 1];
+    }
+    if (tot_a) {
+        S sa = 0, sb = 0;
+        for (int w = 0; w < T / 32; ++w) {
+            sa += scratch[2 * w];
+            sb += scratch[2 * w + 1];
+        }
+        *tot_a = sa;
+        *tot_b = sb;
     }
     a = pa + ia - a;
     b = pb + ib - b;
@@ -264,9 +275,27 @@ __device__ __forceinline__ bool pair_unpack(const Team& tm, int t, const ChainAr
         }
         phase_store_packed<N>(t, words, reinterpret_cast<uint32_t*>(spec));
     } else if (a.dc_window > 0 && a.dc_ref_order) {
-        phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
-        tm.sync();
-        phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);
+        // Integer samples whose row totals stay below 2^24: every partial sum
+        // of the reference's float prefix is an exact integer, so the exact
+        // integer prefix gives the same window sums bit for bit (always the
+        // case for 8-bit samples, and for 12-bit ones up to N = 4096).
+        bool exact = false;
+        if constexpr (DT != IN_F32) {
+            sum_t ta, tb, tot_a, tot_b;
+            phase_dc_local<N, DT>(t, stage, &ta, &tb);
+            team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan, &tot_a, &tot_b);
+            exact = dc_prefix_exact_in_float(tot_a) && dc_prefix_exact_in_float(tot_b);
+            if (exact) {
+                phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
+                tm.sync();
+                phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
+            }
+        }
+        if (!exact) {
+            phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
+            tm.sync();
+            phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);
+        }
     } else if (a.dc_window > 0) {
         sum_t ta, tb;
         phase_dc_local<N, DT>(t, stage, &ta, &tb);

@@ -565,6 +565,11 @@ OPE_HD float sample_as_float(const unsigned char* stage, int n, int row, int i) 
     return (float)x;
 }
 
+// Whether a row total of non-negative integer samples keeps every partial sum
+// of a float prefix exact (below 2^24).
+template <typename S>
+OPE_HD bool dc_prefix_exact_in_float(S total) { return total < (S)16777216; }
+
 // The samples are read in chunks of 32 into registers before the chunk's 32
 // dependent additions: the prefix stores go to shared memory too, so a load
 // after a store could not be issued ahead of it, and each step would wait

@@ -40,6 +40,22 @@ namespace {
 
 enum { OUT_IMAGE = 0, OUT_FFT_INPUT = 1, OUT_BINS = 2, OUT_RESAMPLED = 3 };
 
+// The kernel's reference-order shortcut: integer samples whose two row
+// totals (exact) keep every float partial sum exact take the exact-sum path.
+template <int N, int DT>
+bool ref_order_exact(const unsigned char* stage) {
+    if (DT == IN_F32) return false;
+    using sum_t = typename InTraits<DT>::sum_t;
+    sum_t ta = 0, tb = 0;
+    for (int t = 0; t < N / 16; ++t) {
+        sum_t a, b;
+        phase_dc_local<N, DT>(t, stage, &a, &b);
+        ta += a;
+        tb += b;
+    }
+    return dc_prefix_exact_in_float(ta) && dc_prefix_exact_in_float(tb);
+}
+
 template <int N, int DT, int INTERP>
 int emu_run(const EmuArgs& e, int what, float* out) {
     using PL = Plan<N>;
@@ -143,11 +159,12 @@ int emu_run(const EmuArgs& e, int what, float* out) {
             }
             dc = make_float2(split_level((double)ta, N, DT != IN_F32), split_level((double)tb, N, DT != IN_F32));
             for (int t = 0; t < T; ++t) phase_split_store<N>(t, vals[t].data(), dc, spec);
-        } else if (e.dc_window > 0 && e.dc_ref_order) {
+        } else if (e.dc_window > 0 && e.dc_ref_order && !ref_order_exact<N, DT>(stage.data())) {
             float* pf = reinterpret_cast<float*>(pfx);
             for (int t = 0; t < T; ++t) phase_dc_ref_scan<N, DT>(t, stage.data(), pf);
             for (int t = 0; t < T; ++t) phase_dc_apply<N, DT, true>(t, stage.data(), pf, e.dc_window, spec);
         } else if (e.dc_window > 0) {
+            // exact sums; also the reference order when every float partial sum is exact
             std::vector<sum_t> ta(T), tb(T);
             for (int t = 0; t < T; ++t) phase_dc_local<N, DT>(t, stage.data(), &ta[t], &tb[t]);
             // same order as team_exclusive_scan2: Hillis-Steele inclusive scan per

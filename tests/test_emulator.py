@@ -234,6 +234,28 @@ def test_dc_reference_order_bit_exact_vs_reference_library(emu, reflib, n, dtype
         assert not np.array_equal(y_exact, ref)
 
 
+@pytest.mark.parametrize("bits,dtype", [(12, UINT16), (8, UINT8), (16, UINT16)])
+def test_dc_reference_order_exact_prefix_shortcut(emu, reflib, bits, dtype):
+    """Integer samples whose row totals stay below 2^24 (12-bit samples at
+    N = 2048, any 8-bit ones) take the kernel's exact-prefix shortcut in
+    reference order; the k-linearised spectrum still equals the reference
+    library's bit for bit. One pair mixes a low row with a full-range 16-bit
+    row (totals above 2^24), which takes the serial float prefix instead."""
+    n = 2048
+    spec = spec_for(n, CUBIC, dtype=dtype, m=4, dc_removal=True, dc_window=64, dc_reference_order=True,
+                    dc_split=False)
+    rng = np.random.default_rng(bits)
+    raw = rng.integers(0, 1 << bits, size=(4, n)).astype(np.uint16 if dtype == UINT16 else np.uint8)
+    if dtype == UINT16:
+        raw[3] = rng.integers(30000, 65536, size=n).astype(np.uint16)  # pair (2, 3): one row above 2^24
+    assert (raw[:2].astype(np.int64).sum(axis=1) < (1 << 24)).all() == (bits <= 12)
+    y = H.emu_run(emu, spec, raw, "resampled")
+    r, _, _ = spec.curves()
+    x = np.stack([reflib.convert_input(row, dtype) for row in raw])
+    ref = np.stack([reflib.klinearization(row, r, CUBIC) for row in reflib.rolling_dc(x, 64)])
+    assert np.array_equal(y, ref)
+
+
 @pytest.mark.parametrize("window", [64, 50])
 def test_dc_reference_order_matches_restatement(emu, window):
     """The oracle restatement's rolling mean is the reference's float prefix

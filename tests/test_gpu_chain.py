@@ -58,6 +58,20 @@ def test_dtypes_and_dc_bit_identical_to_emulation(cuda, emu, dtype, dc):
     assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
 
 
+def test_reference_order_exact_prefix_shortcut_bit_identical_to_emulation(cuda, emu):
+    """12-bit samples in reference order: pairs whose row totals stay below
+    2^24 take the exact-prefix shortcut, the pair that mixes in a full-range
+    16-bit row takes the serial float prefix; both equal the emulation (and so
+    the reference library) bit for bit."""
+    spec = spec_for(2048, CUBIC, dtype=UINT16, m=6, dc_removal=True, dc_window=64, dc_reference_order=True)
+    rng = np.random.default_rng(12)
+    raw = rng.integers(0, 4096, size=(6, 2048)).astype(np.uint16)
+    raw[5] = rng.integers(30000, 65536, size=2048).astype(np.uint16)
+    g = H.gpu_run(spec, raw, "bins")
+    e = H.emu_run(emu, spec, raw, "bins")
+    assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
+
+
 @pytest.mark.parametrize("interp", INTERPS)
 @pytest.mark.parametrize("n", [512, 2048, 8192])
 def test_image_vs_oracle(cuda, n, interp):
