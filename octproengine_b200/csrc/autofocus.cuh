@@ -374,8 +374,8 @@ __global__ void __launch_bounds__(N / 16, AfBwdOcc<N>::MIN_BLOCKS) af_backward_k
                 if (!(I.y > 0.0f)) G.y = 0.0f;
                 const float2 g2 = mul2(G, dup2(2.0f));
                 const float2 ure = mul2(g2, x.re), uim = neg2(mul2(g2, x.im));
-                exch[xpad(bin)] = make_float4(ure.x, ure.y, uim.x, uim.y);
-                exch[xpad(bin + N / 2)] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                exch[xslot(bin)] = make_float4(ure.x, ure.y, uim.x, uim.y);
+                exch[xslot(bin + N / 2)] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
         __syncthreads();
         // ---- adjoint DFT: a = F u (all N outputs) ----

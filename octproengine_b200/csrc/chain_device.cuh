@@ -201,6 +201,9 @@ __device__ __forceinline__ void epilogue(const Team& tm, int t, const cp* v, con
                 mn = make_float2(fminf(mn.x, res[k].x), fminf(mn.y, res[k].y));
                 mx = make_float2(fmaxf(mx.x, res[k].x), fmaxf(mx.y, res[k].y));
             }
+            // the scratch may lie inside the exchange buffer, which slower
+            // threads of the team may still be reading in the last pass
+            tm.sync();
             team_minmax2<Plan<N>::T>(tm, mn, mx, scratch);
             float ra = mx.x - mn.x, rb = mx.y - mn.y;
             if (!(ra >= 1e-6f)) ra = 1.0f;
@@ -279,19 +282,37 @@ __device__ __forceinline__ bool pair_unpack(const Team& tm, int t, const ChainAr
         // of the reference's float prefix is an exact integer, so the exact
         // integer prefix gives the same window sums bit for bit (always the
         // case for 8-bit samples, and for 12-bit ones up to N = 4096).
-        bool exact = false;
+        bool done = false;
         if constexpr (DT != IN_F32) {
             sum_t ta, tb, tot_a, tot_b;
             phase_dc_local<N, DT>(t, stage, &ta, &tb);
             team_exclusive_scan2<T, sum_t>(tm, ta, tb, scan, &tot_a, &tot_b);
-            exact = dc_prefix_exact_in_float(tot_a) && dc_prefix_exact_in_float(tot_b);
-            if (exact) {
+            if (dc_prefix_exact_in_float(tot_a) && dc_prefix_exact_in_float(tot_b)) {
                 phase_dc_prefix<N, DT>(t, stage, ta, tb, pfx);
                 tm.sync();
                 phase_dc_apply<N, DT>(t, stage, pfx, a.dc_window, spec);
+                done = true;
+            } else if constexpr (DT == IN_U16) {
+                // the float prefix by segments (phase_dc_refpar_*); the step data
+                // live in the spectrum area, which the apply step writes last
+                int4* seg = reinterpret_cast<int4*>(smem + LY::OFF_SPEC);
+                unsigned* start = reinterpret_cast<unsigned*>(seg + 2 * (N / REFPAR_SEG));
+                float* pf = reinterpret_cast<float*>(pfx);
+                // each segment's four threads take the exact prefix its owner
+                // (thread 4q, the same warp) holds after the scan
+                const int ex_a = __shfl_sync(0xffffffffu, (int)ta, (t & 31) & ~3);
+                const int ex_b = __shfl_sync(0xffffffffu, (int)tb, (t & 31) & ~3);
+                phase_dc_refpar_seg<N>(t, stage, ex_a, ex_b, seg);
+                tm.sync();
+                phase_dc_refpar_walk<N>(t, stage, seg, start);
+                tm.sync();
+                phase_dc_refpar_fill<N>(t, stage, start, pf);
+                tm.sync();
+                phase_dc_apply<N, DT, true>(t, stage, pf, a.dc_window, spec);
+                done = true;
             }
         }
-        if (!exact) {
+        if (!done) {
             phase_dc_ref_scan<N, DT>(t, stage, reinterpret_cast<float*>(pfx));
             tm.sync();
             phase_dc_apply<N, DT, true>(t, stage, pfx, a.dc_window, spec);

@@ -8,7 +8,7 @@
 //   unpack to float pairs (+ rolling-average DC removal)       -> smem "spec"
 //   k-linearisation gather (none / linear / cubic / Lanczos-8)  -> registers
 //   x window x (cos, sin) of the dispersion phase              -> registers
-//   inverse DFT: Stockham radix-16 passes through padded smem  -> registers
+//   inverse DFT: Stockham radix-16 passes through swizzled smem -> registers
 //   FPN subtraction, |X|^2, log10 or linear scaling, affine    -> HBM (bins < N/2)
 //
 // Each raw spectrum is read from HBM once and each output once; everything in
@@ -98,11 +98,17 @@ struct Plan {
     static constexpr int NPASS = (LOG2N + 3) / 4;
     static constexpr int LASTR = 1 << (LOG2N - 4 * (NPASS - 1));
     static constexpr int HALF = N / 2;
-    // padded exchange buffer: one float4 per element plus one per 16
-    static constexpr int EXCH_ELEMS = N + N / 16;
+    // exchange buffer: one float4 per element, slots swizzled by xslot
+    static constexpr int EXCH_ELEMS = N;
 };
 
-OPE_HD int xpad(int e) { return e + (e >> 4); }
+// Exchange-buffer slot of element e: the low three bits (the 16-byte bank
+// group) XORed with bits 4..6. Lanes storing elements 16 apart (the first
+// radix-16 pass) land in distinct bank groups, and runs of 8 consecutive
+// elements (every load, and the stores of later passes) stay conflict-free,
+// with no padding slots: the same bank-group spread as one pad slot per 16
+// elements on every radix schedule, in N slots instead of N + N/16.
+OPE_HD int xslot(int e) { return e ^ ((e >> 4) & 7); }
 
 OPE_HD float bits_f(int b) {
 #if defined(__CUDA_ARCH__)
@@ -595,6 +601,203 @@ OPE_HD void phase_dc_ref_scan(int t, const unsigned char* stage, float* pf) {
     }
 }
 
+// ------------------------ reference-order prefix of 16-bit samples in parallel --
+// The same sequential float prefix, cs[i+1] = fl(cs[i] + x[i]), evaluated by the
+// team instead of one thread per row, bit for bit. It rests on two facts about
+// adding integer samples x to a non-negative float prefix s:
+//  * below 2^24 every partial sum is an exact integer;
+//  * in a binade [2^k, 2^(k+1)) with k >= 24 every float is a multiple of
+//    u = 2^(k-23), and fl(s + x) rounds s/u + x/u to the nearest integer,
+//    ties to even, so the increment in units of u depends only on x and on the
+//    parity of s/u. A run of samples therefore adds the same number of ulps to
+//    every start in the binade with the same parity, as long as no partial
+//    result reaches 2^(k+1).
+// Segments are 64 samples of one row. Step 1: the owner of each segment
+// (thread 4q, which holds the exact integer prefix at sample 64q after the team
+// scan) records the segment's exact sum and, for the binade of that exact
+// prefix, the increments from the starts 2^k (parity 0) and 2^k + u (parity 1),
+// computed with the float additions themselves. Step 2: threads 0 and 1 walk
+// their row's segments in order from 0: exact zone (the segment ends at or
+// below 2^24), one binade step (the walk's value is in the recorded binade and
+// the segment cannot reach the next one), or, for the few segments that cross
+// 2^24 or a binade boundary, the segment's 64 float additions. The walk's value
+// is the prefix as an exact integer (every float below 2^29 is one). Step 3: each
+// owner writes its segment's 64 prefix entries from the segment's start value
+// with the float additions, i.e. exactly the entries of the sequential sum.
+constexpr int REFPAR_SEG = 64;
+
+// Step 1 data per (segment, row) at seg[2*q + row]: {sum, k (-1: below 2^24), d0, d1}.
+OPE_HD int refpar_binade(unsigned v) {  // floor(log2 v), v > 0
+#if defined(__CUDA_ARCH__)
+    return 31 - __clz((int)v);
+#else
+    int k = 0;
+    while (v >> (k + 1)) ++k;
+    return k;
+#endif
+}
+
+OPE_HD unsigned refpar_f2u(float f) {  // an exact integer-valued float < 2^32
+#if defined(__CUDA_ARCH__)
+    return __float2uint_rn(f);
+#else
+    return (unsigned)f;
+#endif
+}
+
+OPE_HD float refpar_u2f(unsigned v) {  // exact for the prefix values (floats below 2^29)
+#if defined(__CUDA_ARCH__)
+    return __uint2float_rn(v);
+#else
+    return (float)v;
+#endif
+}
+
+// Samples [8k, 8k + 8) of segment q of row `row` as exact floats, read as one
+// 16-byte word. On the device each float is 2^23 + x, built by a byte permute,
+// minus 2^23 (exact): conversion instructions run at a fraction of the FP32
+// rate, and the few threads of a segment step would spend most of their time
+// in them.
+template <int N>
+OPE_HD void refpar_load8(const unsigned char* stage, int row, int q, int k, float* x) {
+    const unsigned short* p = reinterpret_cast<const unsigned short*>(stage) + row * N + REFPAR_SEG * q + 8 * k;
+#if defined(__CUDA_ARCH__)
+    const uint4 w = *reinterpret_cast<const uint4*>(p);
+    const unsigned v[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        x[2 * j] = fsub_rn(__uint_as_float(__byte_perm(v[j], 0x4B00u, 0x5410)), 8388608.0f);
+        x[2 * j + 1] = fsub_rn(__uint_as_float(__byte_perm(v[j], 0x4B00u, 0x5432)), 8388608.0f);
+    }
+#else
+    for (int j = 0; j < 8; ++j) x[j] = (float)p[j];
+#endif
+}
+
+// Step 1. Segment q's four threads 4q .. 4q+3 each run one (row, parity)
+// chain: thread 4q + 2r + p adds the segment's samples of row r to the start
+// 2^k + p*u of the binade k of the row's exact prefix at the segment start
+// (ex_a / ex_b: the values thread 4q holds after the team scan); the p = 0
+// thread also records the segment's exact sum (exact in float: below 2^24) and k.
+template <int N>
+OPE_HD void phase_dc_refpar_seg(int t, const unsigned char* stage, int ex_a, int ex_b, int4* seg) {
+    static_assert(N % REFPAR_SEG == 0 && 4 * (N / REFPAR_SEG) <= N / 16, "four threads per 64-sample segment");
+    const int q = t >> 2, r = (t >> 1) & 1, par = t & 1;
+    const unsigned ex = (unsigned)(r ? ex_b : ex_a);
+    const bool binade = ex >= (1u << 24);
+    if (!binade && par) return;
+    const int k = binade ? refpar_binade(ex) : -1;
+    const int sh = k - 23;
+    const unsigned b = binade ? (1u << k) + ((unsigned)par << sh) : 0u;
+    float s = refpar_u2f(b), sum = 0.0f;
+#pragma unroll
+    for (int c = 0; c < REFPAR_SEG / 8; ++c) {
+        float x[8];
+        refpar_load8<N>(stage, r, q, c, x);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (binade) s = fadd_rn(s, x[i]);
+            if (!par) sum = fadd_rn(sum, x[i]);
+        }
+    }
+    OPE_SMEM_CHECK(2 * q + r < 2 * (N / REFPAR_SEG));
+    int* g = reinterpret_cast<int*>(&seg[2 * q + r]);
+    const int d = binade ? (int)((refpar_f2u(s) - b) >> sh) : 0;
+    if (par) {
+        g[3] = d;
+    } else {
+        g[0] = (int)refpar_f2u(sum);
+        g[1] = k;
+        g[2] = d;
+        if (!binade) g[3] = 0;  // no parity-1 chain for this segment
+    }
+}
+
+// The 64 float additions of segment q of row `row` onto f (out of line on the
+// device: the walk needs it for a few segments per row only).
+template <int N>
+#if defined(__CUDACC__)
+__host__ __device__ __noinline__
+#else
+inline
+#endif
+float refpar_add_segment(const unsigned char* stage, int row, int q, float f) {
+    float x[REFPAR_SEG];
+#pragma unroll
+    for (int c = 0; c < REFPAR_SEG / 8; ++c) refpar_load8<N>(stage, row, q, c, x + 8 * c);
+#pragma unroll
+    for (int i = 0; i < REFPAR_SEG; ++i) f = fadd_rn(f, x[i]);
+    return f;
+}
+
+// Step 2. Row 0 is walked by thread 0 and row 1 by thread 32 (lane 1 when the
+// team is one warp), so that a segment one row adds up sample by sample does
+// not hold up the other row's walk. The step records are read in blocks of 8
+// ahead of the block's steps.
+template <int N>
+OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, const int4* seg, unsigned* start) {
+    constexpr int WALKER1 = Plan<N>::T >= 64 ? 32 : 1;
+    if (t != 0 && t != WALKER1) return;
+    const int r = t == 0 ? 0 : 1;
+    constexpr int NSEG = N / REFPAR_SEG;
+    constexpr int B = NSEG < 8 ? NSEG : 8;
+    static_assert(NSEG % B == 0, "whole blocks of segments");
+    unsigned s = 0;
+#pragma unroll 1
+    for (int q0 = 0; q0 < NSEG; q0 += B) {
+        int4 g[B];
+        unsigned st[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) g[j] = seg[2 * (q0 + j) + r];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            st[j] = s;
+            const unsigned end = s + (unsigned)g[j].x;
+            bool stepped = false;
+            if (end <= (1u << 24)) {  // every partial sum exact
+                s = end;
+                stepped = true;
+            } else if (s >= (1u << 24)) {
+                const int k = refpar_binade(s);
+                const int sh = k - 23;
+                // 64 roundings add at most 32 ulps beyond the exact segment sum
+                if (k == g[j].y && end + (32u << sh) < (2u << k)) {
+                    s += (unsigned)(((s >> sh) & 1u) ? g[j].w : g[j].z) << sh;
+                    stepped = true;
+                }
+            }
+            if (!stepped) s = refpar_f2u(refpar_add_segment<N>(stage, r, q0 + j, refpar_u2f(s)));
+        }
+#pragma unroll
+        for (int j = 0; j < B; ++j) start[2 * (q0 + j) + r] = st[j];
+    }
+}
+
+// Step 3. Threads 4q and 4q + 1 write rows 0 and 1 of segment q: the 64
+// prefix entries from the segment's start value, with the float additions.
+template <int N>
+OPE_HD void phase_dc_refpar_fill(int t, const unsigned char* stage, const unsigned* start, float* pf) {
+    if ((t & 3) > 1) return;
+    const int q = t >> 2, r = t & 1;
+    if (t == 0) {
+        pf[pfx_idx(0)] = 0.0f;
+        pf[pfx_idx(1)] = 0.0f;
+    }
+    float s = refpar_u2f(start[2 * q + r]);
+#pragma unroll
+    for (int c = 0; c < REFPAR_SEG / 8; ++c) {
+        float x[8];
+        refpar_load8<N>(stage, r, q, c, x);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = REFPAR_SEG * q + 8 * c + i + 1;
+            s = fadd_rn(s, x[i]);
+            OPE_SMEM_CHECK(pfx_idx(2 * e + r) < pfx_idx(2 * (N + 1)));
+            pf[pfx_idx(2 * e + r)] = s;
+        }
+    }
+}
+
 // Step C: subtract the window means and write the spectrum pairs. A window of
 // a power-of-two count (the interior, when 2W is one: W = 64 by default) is
 // divided by multiplying with its exact reciprocal, which equals the correctly
@@ -854,8 +1057,8 @@ OPE_HD void fft_load(int t, const float4* exch, cp* v) {
 #pragma unroll
     for (int s = 0; s < 16; ++s) {
         int e = t + s * T;
-        OPE_SMEM_CHECK(xpad(e) < Plan<N>::EXCH_ELEMS);
-        float4 q = exch[xpad(e)];
+        OPE_SMEM_CHECK(xslot(e) < Plan<N>::EXCH_ELEMS);
+        float4 q = exch[xslot(e)];
         v[s] = cpmake(make_float2(q.x, q.y), make_float2(q.z, q.w));
     }
 }
@@ -910,9 +1113,9 @@ OPE_HD void fft_store(int t, const cp* v, float4* exch) {
 #pragma unroll
         for (int q = 0; q < R; ++q) {
             int e = base + q * NS;
-            OPE_SMEM_CHECK(e >= 0 && e < N && xpad(e) < Plan<N>::EXCH_ELEMS);
+            OPE_SMEM_CHECK(e >= 0 && e < N && xslot(e) < Plan<N>::EXCH_ELEMS);
             cp x = v[i + q * D];
-            exch[xpad(e)] = make_float4(x.re.x, x.re.y, x.im.x, x.im.y);
+            exch[xslot(e)] = make_float4(x.re.x, x.re.y, x.im.x, x.im.y);
         }
     }
 }

@@ -161,7 +161,27 @@ int emu_run(const EmuArgs& e, int what, float* out) {
             for (int t = 0; t < T; ++t) phase_split_store<N>(t, vals[t].data(), dc, spec);
         } else if (e.dc_window > 0 && e.dc_ref_order && !ref_order_exact<N, DT>(stage.data())) {
             float* pf = reinterpret_cast<float*>(pfx);
-            for (int t = 0; t < T; ++t) phase_dc_ref_scan<N, DT>(t, stage.data(), pf);
+            if constexpr (DT == IN_U16) {
+                // the kernel's segment form of the float prefix: exact integer
+                // prefixes per thread (any order), then its three steps in turn
+                std::vector<int> ta(T), tb(T);
+                int pa = 0, pb = 0;
+                for (int t = 0; t < T; ++t) {
+                    int a0, b0;
+                    phase_dc_local<N, DT>(t, stage.data(), &a0, &b0);
+                    ta[t] = pa;
+                    tb[t] = pb;
+                    pa += a0;
+                    pb += b0;
+                }
+                int4* seg = reinterpret_cast<int4*>(work.data() + LY::OFF_SPEC);
+                unsigned* start = reinterpret_cast<unsigned*>(seg + 2 * (N / REFPAR_SEG));
+                for (int t = 0; t < T; ++t) phase_dc_refpar_seg<N>(t, stage.data(), ta[t & ~3], tb[t & ~3], seg);
+                for (int t = 0; t < T; ++t) phase_dc_refpar_walk<N>(t, stage.data(), seg, start);
+                for (int t = 0; t < T; ++t) phase_dc_refpar_fill<N>(t, stage.data(), start, pf);
+            } else {
+                for (int t = 0; t < T; ++t) phase_dc_ref_scan<N, DT>(t, stage.data(), pf);
+            }
             for (int t = 0; t < T; ++t) phase_dc_apply<N, DT, true>(t, stage.data(), pf, e.dc_window, spec);
         } else if (e.dc_window > 0) {
             // exact sums; also the reference order when every float partial sum is exact

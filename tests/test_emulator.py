@@ -256,6 +256,31 @@ def test_dc_reference_order_exact_prefix_shortcut(emu, reflib, bits, dtype):
     assert np.array_equal(y, ref)
 
 
+@pytest.mark.parametrize("n", [2048, 8192])
+def test_dc_reference_order_segments_bit_exact_on_structured_rows(emu, reflib, n):
+    """16-bit samples in reference order take the kernel's segment form of the
+    float prefix (per-binade parity steps, float additions across 2^24 and the
+    binade boundaries). Rows built to stress it: constant 65535 (the sum ends
+    in the 2^28 binade at N = 8192), constant 32769 (an odd sample: every
+    addition in the 2-ulp binade is a tie), alternating 65535 / 1, values
+    2 mod 4 near the top (ties in the 4-ulp binade), a full-range random row
+    and a high-range one. The k-linearised spectrum equals the reference
+    library's convertInput -> rollingAverageDCRemoval -> kLinearization bit
+    for bit (cpu_kernels.tpp:24-82,113-146)."""
+    rng = np.random.default_rng(n)
+    i = np.arange(n)
+    raw = np.stack([np.full(n, 65535), np.full(n, 32769), np.where(i % 2 == 1, 65535, 1),
+                    65530 - 4 * rng.integers(0, 8, size=n), rng.integers(0, 65536, size=n),
+                    rng.integers(30000, 65536, size=n)]).astype(np.uint16)
+    spec = spec_for(n, CUBIC, dtype=UINT16, m=raw.shape[0], dc_removal=True, dc_window=64,
+                    dc_reference_order=True, dc_split=False)
+    y = H.emu_run(emu, spec, raw, "resampled")
+    r, _, _ = spec.curves()
+    x = np.stack([reflib.convert_input(row, UINT16) for row in raw])
+    ref = np.stack([reflib.klinearization(row, r, CUBIC) for row in reflib.rolling_dc(x, 64)])
+    assert np.array_equal(y, ref)
+
+
 @pytest.mark.parametrize("window", [64, 50])
 def test_dc_reference_order_matches_restatement(emu, window):
     """The oracle restatement's rolling mean is the reference's float prefix
