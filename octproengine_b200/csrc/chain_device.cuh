@@ -295,18 +295,18 @@ __device__ __forceinline__ bool pair_unpack(const Team& tm, int t, const ChainAr
             } else if constexpr (DT == IN_U16) {
                 // the float prefix by segments (phase_dc_refpar_*); the step data
                 // live in the spectrum area, which the apply step writes last
-                int4* seg = reinterpret_cast<int4*>(smem + LY::OFF_SPEC);
-                unsigned* start = reinterpret_cast<unsigned*>(seg + 2 * (N / REFPAR_SEG));
+                static_assert(RefparArea<N>::BYTES <= LY::SPEC_BYTES, "the step records fit the spectrum area");
+                unsigned char* area = smem + LY::OFF_SPEC;
                 float* pf = reinterpret_cast<float*>(pfx);
                 // each segment's four threads take the exact prefix its owner
                 // (thread 4q, the same warp) holds after the scan
                 const int ex_a = __shfl_sync(0xffffffffu, (int)ta, (t & 31) & ~3);
                 const int ex_b = __shfl_sync(0xffffffffu, (int)tb, (t & 31) & ~3);
-                phase_dc_refpar_seg<N>(t, stage, ex_a, ex_b, seg);
+                phase_dc_refpar_seg<N>(t, stage, ex_a, ex_b, area);
                 tm.sync();
-                phase_dc_refpar_walk<N>(t, stage, seg, start);
+                phase_dc_refpar_walk<N>(t, stage, area);
                 tm.sync();
-                phase_dc_refpar_fill<N>(t, stage, start, pf);
+                phase_dc_refpar_fill<N>(t, stage, area, pf);
                 tm.sync();
                 phase_dc_apply<N, DT, true>(t, stage, pf, a.dc_window, spec);
                 done = true;

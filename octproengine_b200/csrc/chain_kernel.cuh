@@ -137,10 +137,10 @@ struct Layout {
     using sum_t = typename InTraits<DT>::sum_t;
     using raw_t = typename InTraits<DT>::raw_t;
     static constexpr int SPEC_BYTES = (N + 2 * SPEC_PAD) * 8;        // float2 pairs
-    // prefix sums, 2 rows, one pad word per 32 (pfx_idx): conflict-free writes and reads;
+    // prefix sums, 2 rows, two pad words per 32 (pfx_idx): conflict-free writes and reads;
     // rounded to 16 bytes so that the scan scratch after it holds doubles aligned
     static constexpr int PFX_BYTES =
-        (((N + 1) * 2 + ((N + 1) * 2) / 32 + 1) * (int)sizeof(sum_t) + 15) / 16 * 16;
+        (((N + 1) * 2 + 2 * (((N + 1) * 2) / 32) + 2) * (int)sizeof(sum_t) + 15) / 16 * 16;
     static constexpr int EXCH_BYTES_RAW = Plan<N>::EXCH_ELEMS * 16;
     static constexpr int WORK_BYTES = (EXCH_BYTES_RAW > SPEC_BYTES + PFX_BYTES + 256)
                                           ? EXCH_BYTES_RAW
@@ -458,10 +458,17 @@ OPE_HD void phase_bitshift(int t, unsigned char* stage) {
 // (the reference accumulates them in float; for integer input whose running
 // sum stays below 2^24 both are identical).
 //
-// Prefix-sum word w (2*i + row) lives at pfx_idx(w): one pad word per 32 puts
+// Prefix-sum word w (2*i + row) lives at pfx_idx(w): two pad words per 32 put
 // the 16-sample segments of consecutive threads, and the window ends that
-// consecutive threads read, in distinct banks.
-OPE_HD int pfx_idx(int w) { return w + (w >> 5); }
+// consecutive threads read, in distinct banks, and keep the two rows' entries of
+// sample i (words 2i, 2i + 1) one aligned pair, read and written together.
+OPE_HD int pfx_idx(int w) { return w + 2 * (w >> 5); }
+
+// The two rows' prefix entries of one sample, as one aligned pair.
+template <typename S>
+struct PfxPair {
+    S a, b;
+};
 
 // The 16 samples [16t, 16t+16) of both rows, widened to the sum type (device:
 // 16-byte shared loads).
@@ -547,8 +554,7 @@ OPE_HD void phase_dc_prefix(int t, const unsigned char* stage, typename InTraits
         sa += xa[k];
         sb += xb[k];
         OPE_SMEM_CHECK(pfx_idx(2 * (i + 1) + 1) < pfx_idx(2 * (N + 1)));
-        pfx[pfx_idx(2 * (i + 1))] = sa;
-        pfx[pfx_idx(2 * (i + 1) + 1)] = sb;
+        *reinterpret_cast<PfxPair<sum_t>*>(&pfx[pfx_idx(2 * (i + 1))]) = PfxPair<sum_t>{sa, sb};
     }
 }
 
@@ -612,21 +618,20 @@ OPE_HD void phase_dc_ref_scan(int t, const unsigned char* stage, float* pf) {
 //    parity of s/u. A run of samples therefore adds the same number of ulps to
 //    every start in the binade with the same parity, as long as no partial
 //    result reaches 2^(k+1).
-// Segments are 64 samples of one row. Step 1: the owner of each segment
-// (thread 4q, which holds the exact integer prefix at sample 64q after the team
-// scan) records the segment's exact sum and, for the binade of that exact
-// prefix, the increments from the starts 2^k (parity 0) and 2^k + u (parity 1),
-// computed with the float additions themselves. Step 2: threads 0 and 1 walk
-// their row's segments in order from 0: exact zone (the segment ends at or
-// below 2^24), one binade step (the walk's value is in the recorded binade and
-// the segment cannot reach the next one), or, for the few segments that cross
-// 2^24 or a binade boundary, the segment's 64 float additions. The walk's value
-// is the prefix as an exact integer (every float below 2^29 is one). Step 3: each
-// owner writes its segment's 64 prefix entries from the segment's start value
-// with the float additions, i.e. exactly the entries of the sequential sum.
+// Segments are 64 samples of one row, split into four 16-sample parts. Step 1:
+// each segment's four threads build step records (refpar_step) for its parts in
+// the binade of the row's exact integer prefix at the segment start and in the
+// next binade, with the float additions from synthetic starts, and compose the
+// first set into the whole segment's record. Step 2: threads 0 and 32 walk their
+// row's segments in order from 0, one record per segment; a segment whose record
+// does not apply (it crosses 2^24 or a binade boundary, or the walk's value lies
+// in another binade than the exact prefix) is walked part by part, and only a
+// part that itself crosses is added sample by sample. The walk's value is the
+// prefix as an exact integer (every float below 2^30 is one). Step 3: the four
+// threads write the segment's 64 prefix entries from its start value with the
+// float additions, i.e. exactly the entries of the sequential sum.
 constexpr int REFPAR_SEG = 64;
 
-// Step 1 data per (segment, row) at seg[2*q + row]: {sum, k (-1: below 2^24), d0, d1}.
 OPE_HD int refpar_binade(unsigned v) {  // floor(log2 v), v > 0
 #if defined(__CUDA_ARCH__)
     return 31 - __clz((int)v);
@@ -674,72 +679,143 @@ OPE_HD void refpar_load8(const unsigned char* stage, int row, int q, int k, floa
 #endif
 }
 
-// Step 1. Segment q's four threads 4q .. 4q+3 each run one (row, parity)
-// chain: thread 4q + 2r + p adds the segment's samples of row r to the start
-// 2^k + p*u of the binade k of the row's exact prefix at the segment start
-// (ex_a / ex_b: the values thread 4q holds after the team scan); the p = 0
-// thread also records the segment's exact sum (exact in float: below 2^24) and k.
-template <int N>
-OPE_HD void phase_dc_refpar_seg(int t, const unsigned char* stage, int ex_a, int ex_b, int4* seg) {
-    static_assert(N % REFPAR_SEG == 0 && 4 * (N / REFPAR_SEG) <= N / 16, "four threads per 64-sample segment");
-    const int q = t >> 2, r = (t >> 1) & 1, par = t & 1;
-    const unsigned ex = (unsigned)(r ? ex_b : ex_a);
-    const bool binade = ex >= (1u << 24);
-    if (!binade && par) return;
-    const int k = binade ? refpar_binade(ex) : -1;
+// A step record {hi, u, d0 * u, d1 * u}: for a prefix value s (an exact
+// integer) with u << 23 <= s < hi, the run of samples takes s to s + d0 * u if
+// s / u is even and to s + d1 * u if it is odd. For a binade k >= 24, u = 2^(k-23)
+// and hi = 2^(k+1) - (the run's exact sum) - (its roundings' bound): the run
+// stays in the binade. For the exact zone u = 0, hi = 2^24 - sum + 1 and
+// d0 = d1 = sum: every partial sum stays an exact integer.
+OPE_HD bool refpar_step(unsigned& s, int4 g) {
+    const unsigned u = (unsigned)g.y;
+    if (s < (u << 23) || s >= (unsigned)g.x) return false;
+    s += (unsigned)((s & u) ? g.w : g.z);
+    return true;
+}
+
+// Record of a run with exact sum `sum`, in binade k (k < 24: the exact zone),
+// from its increments d0, d1 (in ulps) and the run's length in samples.
+OPE_HD int4 refpar_record(int k, unsigned sum, int d0, int d1, int len) {
+    if (k < 24) return make_int4((int)((1u << 24) - sum + 1u), 0, (int)sum, (int)sum);
     const int sh = k - 23;
-    const unsigned b = binade ? (1u << k) + ((unsigned)par << sh) : 0u;
-    float s = refpar_u2f(b), sum = 0.0f;
+    const unsigned u = 1u << sh;
+    return make_int4((int)((2u << k) - sum - (unsigned)(len / 2) * u), (int)u, d0 << sh, d1 << sh);
+}
+
+// Shared-memory areas of the three steps (in the spectrum area, which the
+// window-mean step writes last): per (segment q, row r), index 2q + r, the
+// segment's record for the binade of its exact prefix; the records of its four
+// 16-sample parts for that binade and for the next one (8 per index); and the
+// segment's start value.
+template <int N>
+struct RefparArea {
+    static constexpr int NSEG = N / REFPAR_SEG;
+    int4* seg;
+    int4* part;
+    unsigned* start;
+    OPE_HD explicit RefparArea(unsigned char* base)
+        : seg(reinterpret_cast<int4*>(base)),
+          part(reinterpret_cast<int4*>(base) + 2 * NSEG),
+          start(reinterpret_cast<unsigned*>(reinterpret_cast<int4*>(base) + 2 * NSEG * 9)) {}
+    static constexpr int BYTES = 2 * NSEG * (9 * 16 + 4);
+};
+
+// Step 1. Segment q's four threads 4q .. 4q+3: thread 4q + 2r + b builds, for
+// row r, the records of the segment's four 16-sample parts in binade k + b, k the
+// binade of the row's exact prefix at the segment start (ex_a / ex_b: the values
+// thread 4q holds after the team scan; the exact zone counts as binade 23, its
+// next one is 24), with the float additions from the starts 2^k' and 2^k' + u of
+// that binade; the b = 0 thread also composes them into the whole segment's record.
+template <int N>
+OPE_HD void phase_dc_refpar_seg(int t, const unsigned char* stage, int ex_a, int ex_b, unsigned char* area) {
+    static_assert(N % REFPAR_SEG == 0 && 4 * (N / REFPAR_SEG) <= N / 16, "four threads per 64-sample segment");
+    const RefparArea<N> A(area);
+    const int q = t >> 2, r = (t >> 1) & 1, b = t & 1;
+    const unsigned ex = (unsigned)(r ? ex_b : ex_a);
+    const int k0 = ex >= (1u << 24) ? refpar_binade(ex) : 23;
+    const int k = k0 + b;
+    const int sh = k - 23;
+    const unsigned base = 1u << k;
+    const float s0_init = refpar_u2f(base), s1_init = refpar_u2f(base + (1u << sh));
+    int d0[4], d1[4];
+    unsigned sums[4];
+    int4* part = A.part + 8 * (2 * q + r);
 #pragma unroll
-    for (int c = 0; c < REFPAR_SEG / 8; ++c) {
-        float x[8];
-        refpar_load8<N>(stage, r, q, c, x);
+    for (int j = 0; j < 4; ++j) {
+        float x[16];
+        refpar_load8<N>(stage, r, q, 2 * j, x);
+        refpar_load8<N>(stage, r, q, 2 * j + 1, x + 8);
+        float s0 = s0_init, s1 = s1_init, sum = 0.0f;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (binade) s = fadd_rn(s, x[i]);
-            if (!par) sum = fadd_rn(sum, x[i]);
+        for (int i = 0; i < 16; ++i) {
+            s0 = fadd_rn(s0, x[i]);
+            s1 = fadd_rn(s1, x[i]);
+            sum = fadd_rn(sum, x[i]);  // exact: below 2^24
         }
+        sums[j] = refpar_f2u(sum);
+        d0[j] = (int)((refpar_f2u(s0) - base) >> sh);
+        d1[j] = (int)((refpar_f2u(s1) - base - (1u << sh)) >> sh);
+        part[2 * j + b] = refpar_record(k, sums[j], d0[j], d1[j], 16);
     }
-    OPE_SMEM_CHECK(2 * q + r < 2 * (N / REFPAR_SEG));
-    int* g = reinterpret_cast<int*>(&seg[2 * q + r]);
-    const int d = binade ? (int)((refpar_f2u(s) - b) >> sh) : 0;
-    if (par) {
-        g[3] = d;
-    } else {
-        g[0] = (int)refpar_f2u(sum);
-        g[1] = k;
-        g[2] = d;
-        if (!binade) g[3] = 0;  // no parity-1 chain for this segment
+    if (b == 0) {
+        // the parts composed: the parity after a part of d ulps flips with d's parity
+        int inc[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            int acc = 0, par = p;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int d = par ? d1[j] : d0[j];
+                acc += d;
+                par ^= d & 1;
+            }
+            inc[p] = acc;
+        }
+        OPE_SMEM_CHECK(2 * q + r < 2 * (N / REFPAR_SEG));
+        A.seg[2 * q + r] = refpar_record(k, sums[0] + sums[1] + sums[2] + sums[3], inc[0], inc[1], REFPAR_SEG);
     }
 }
 
-// The 64 float additions of segment q of row `row` onto f (out of line on the
-// device: the walk needs it for a few segments per row only).
+// The float additions of samples [16j, 16j + 16) of segment q of row `row` onto f
+// (out of line on the device: the walk needs it for a few parts per row only).
 template <int N>
 #if defined(__CUDACC__)
 __host__ __device__ __noinline__
 #else
 inline
 #endif
-float refpar_add_segment(const unsigned char* stage, int row, int q, float f) {
-    float x[REFPAR_SEG];
+float refpar_add_part(const unsigned char* stage, int row, int q, int j, float f) {
+    float x[16];
+    refpar_load8<N>(stage, row, q, 2 * j, x);
+    refpar_load8<N>(stage, row, q, 2 * j + 1, x + 8);
 #pragma unroll
-    for (int c = 0; c < REFPAR_SEG / 8; ++c) refpar_load8<N>(stage, row, q, c, x + 8 * c);
-#pragma unroll
-    for (int i = 0; i < REFPAR_SEG; ++i) f = fadd_rn(f, x[i]);
+    for (int i = 0; i < 16; ++i) f = fadd_rn(f, x[i]);
     return f;
 }
 
-// Step 2. Row 0 is walked by thread 0 and row 1 by thread 32 (lane 1 when the
-// team is one warp), so that a segment one row adds up sample by sample does
-// not hold up the other row's walk. The step records are read in blocks of 8
-// ahead of the block's steps.
+// A segment whose record does not apply (it crosses 2^24 or a binade boundary,
+// or the walk's value is not in the binade of the exact prefix): its four parts,
+// each by its record for the segment's binade or the next one, or, for the part
+// that crosses, by its 16 float additions.
 template <int N>
-OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, const int4* seg, unsigned* start) {
+OPE_HD unsigned refpar_walk_parts(const unsigned char* stage, const int4* part, int row, int q, unsigned s) {
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+        if (refpar_step(s, part[2 * j]) || refpar_step(s, part[2 * j + 1])) continue;
+        s = refpar_f2u(refpar_add_part<N>(stage, row, q, j, refpar_u2f(s)));
+    }
+    return s;
+}
+
+// Step 2. Row 0 is walked by thread 0 and row 1 by thread 32 (lane 1 when the
+// team is one warp), so that the rows' part-wise segments do not hold up each
+// other. The segment records are read in blocks of 8 ahead of the block's steps.
+template <int N>
+OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, unsigned char* area) {
     constexpr int WALKER1 = Plan<N>::T >= 64 ? 32 : 1;
     if (t != 0 && t != WALKER1) return;
+    const RefparArea<N> A(area);
     const int r = t == 0 ? 0 : 1;
-    constexpr int NSEG = N / REFPAR_SEG;
+    constexpr int NSEG = RefparArea<N>::NSEG;
     constexpr int B = NSEG < 8 ? NSEG : 8;
     static_assert(NSEG % B == 0, "whole blocks of segments");
     unsigned s = 0;
@@ -748,49 +824,45 @@ OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, const int4* 
         int4 g[B];
         unsigned st[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j) g[j] = seg[2 * (q0 + j) + r];
+        for (int j = 0; j < B; ++j) g[j] = A.seg[2 * (q0 + j) + r];
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             st[j] = s;
-            const unsigned end = s + (unsigned)g[j].x;
-            bool stepped = false;
-            if (end <= (1u << 24)) {  // every partial sum exact
-                s = end;
-                stepped = true;
-            } else if (s >= (1u << 24)) {
-                const int k = refpar_binade(s);
-                const int sh = k - 23;
-                // 64 roundings add at most 32 ulps beyond the exact segment sum
-                if (k == g[j].y && end + (32u << sh) < (2u << k)) {
-                    s += (unsigned)(((s >> sh) & 1u) ? g[j].w : g[j].z) << sh;
-                    stepped = true;
-                }
-            }
-            if (!stepped) s = refpar_f2u(refpar_add_segment<N>(stage, r, q0 + j, refpar_u2f(s)));
+            if (!refpar_step(s, g[j])) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * (q0 + j) + r), r, q0 + j, s);
         }
 #pragma unroll
-        for (int j = 0; j < B; ++j) start[2 * (q0 + j) + r] = st[j];
+        for (int j = 0; j < B; ++j) A.start[2 * (q0 + j) + r] = st[j];
     }
 }
 
-// Step 3. Threads 4q and 4q + 1 write rows 0 and 1 of segment q: the 64
-// prefix entries from the segment's start value, with the float additions.
+// Step 3. Segment q's four threads write its prefix entries: thread 4q + 2r + h
+// the 32 entries of half h of row r, from the segment's start value (half 1: after
+// the first two parts, by their records or their additions), with the float
+// additions.
 template <int N>
-OPE_HD void phase_dc_refpar_fill(int t, const unsigned char* stage, const unsigned* start, float* pf) {
-    if ((t & 3) > 1) return;
-    const int q = t >> 2, r = t & 1;
+OPE_HD void phase_dc_refpar_fill(int t, const unsigned char* stage, unsigned char* area, float* pf) {
+    const RefparArea<N> A(area);
+    const int q = t >> 2, r = (t >> 1) & 1, h = t & 1;
     if (t == 0) {
         pf[pfx_idx(0)] = 0.0f;
         pf[pfx_idx(1)] = 0.0f;
     }
-    float s = refpar_u2f(start[2 * q + r]);
+    unsigned s0 = A.start[2 * q + r];
+    if (h) {
+        const int4* part = A.part + 8 * (2 * q + r);
+#pragma unroll 1
+        for (int j = 0; j < 2; ++j)
+            if (!refpar_step(s0, part[2 * j]) && !refpar_step(s0, part[2 * j + 1]))
+                s0 = refpar_f2u(refpar_add_part<N>(stage, r, q, j, refpar_u2f(s0)));
+    }
+    float s = refpar_u2f(s0);
 #pragma unroll
-    for (int c = 0; c < REFPAR_SEG / 8; ++c) {
+    for (int c = 0; c < 4; ++c) {
         float x[8];
-        refpar_load8<N>(stage, r, q, c, x);
+        refpar_load8<N>(stage, r, q, 4 * h + c, x);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const int e = REFPAR_SEG * q + 8 * c + i + 1;
+            const int e = REFPAR_SEG * q + 32 * h + 8 * c + i + 1;
             s = fadd_rn(s, x[i]);
             OPE_SMEM_CHECK(pfx_idx(2 * e + r) < pfx_idx(2 * (N + 1)));
             pf[pfx_idx(2 * e + r)] = s;
@@ -805,6 +877,15 @@ OPE_HD void phase_dc_refpar_fill(int t, const unsigned char* stage, const unsign
 // REF = false: exact window sums from the integer prefix sums of
 // phase_dc_prefix; REF = true: the reference's float difference of two entries
 // of the sequential float prefix sum (phase_dc_ref_scan).
+//
+// Chunks of 8 samples whose windows all hold 2W samples (the interior), when 2W
+// is a power of two, take a short path: both rows' prefix entries of a window
+// end as one pair, the two window sums and means as float pairs, and for 8/16-bit
+// samples whose window sums stay below 2^23 the sums converted exactly as
+// (2^23 + S) - 2^23 (the bits of 2^23 + S are those of 2^23 with S in the
+// mantissa) instead of by conversion instructions. Same values as the general
+// path: the sums are exact integers below 2^24 either way, and the products with
+// 1/(2W) are exact.
 template <int N, int DT, bool REF = false>
 OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const void* pfx_v, int W, float2* spec) {
     using sum_t = typename InTraits<DT>::sum_t;
@@ -812,10 +893,38 @@ OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const void* pfx_v,
     const int full = 2 * W;
     const bool full_pow2 = (full & (full - 1)) == 0;
     const float full_inv = 1.0f / (float)full;  // exact when full is a power of two
-#pragma unroll
+    constexpr int MAXV = DT == IN_U8 ? 255 : 65535;
+    const bool bias_sum = (DT == IN_U8 || DT == IN_U16) && (long long)full * MAXV < 8388608LL;
+    // not unrolled: two copies of the chunk body cost more in instruction
+    // fetch than the loop (measured: 90 against 107 M A-scans/s at N = 2048)
+#pragma unroll 1
     for (int c = t; c < N / 8; c += T) {
         float2 v[8];
         load_chunk8<DT>(stage, N, c, v);
+        if (full_pow2 && 8 * c >= W - 1 && 8 * c + 7 + W < N - 1) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int i = 8 * c + k;
+                const int hi = pfx_idx(2 * (i + W + 1)), lo = pfx_idx(2 * (i - W + 1));
+                float2 sum;
+                if constexpr (REF) {
+                    const float* pf = static_cast<const float*>(pfx_v);
+                    sum = sub2(*reinterpret_cast<const float2*>(&pf[hi]), *reinterpret_cast<const float2*>(&pf[lo]));
+                } else {
+                    const sum_t* pfx = static_cast<const sum_t*>(pfx_v);
+                    const PfxPair<sum_t> ph = *reinterpret_cast<const PfxPair<sum_t>*>(&pfx[hi]);
+                    const PfxPair<sum_t> pl = *reinterpret_cast<const PfxPair<sum_t>*>(&pfx[lo]);
+                    const sum_t da = ph.a - pl.a, db = ph.b - pl.b;
+                    if (bias_sum)
+                        sum = sub2(make_float2(bits_f((int)(0x4B000000u | (unsigned)da)),
+                                               bits_f((int)(0x4B000000u | (unsigned)db))),
+                                   dup2(8388608.0f));
+                    else
+                        sum = make_float2((float)da, (float)db);
+                }
+                v[k] = sub2(v[k], mul2(sum, dup2(full_inv)));
+            }
+        } else {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             int i = 8 * c + k;
@@ -847,6 +956,7 @@ OPE_HD void phase_dc_apply(int t, const unsigned char* stage, const void* pfx_v,
 #endif
             }
             v[k] = sub2(v[k], make_float2(ma, mb));
+        }
         }
 #pragma unroll
         for (int i = 0; i < 8; i += 2)

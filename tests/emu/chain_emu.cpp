@@ -174,11 +174,11 @@ int emu_run(const EmuArgs& e, int what, float* out) {
                     pa += a0;
                     pb += b0;
                 }
-                int4* seg = reinterpret_cast<int4*>(work.data() + LY::OFF_SPEC);
-                unsigned* start = reinterpret_cast<unsigned*>(seg + 2 * (N / REFPAR_SEG));
-                for (int t = 0; t < T; ++t) phase_dc_refpar_seg<N>(t, stage.data(), ta[t & ~3], tb[t & ~3], seg);
-                for (int t = 0; t < T; ++t) phase_dc_refpar_walk<N>(t, stage.data(), seg, start);
-                for (int t = 0; t < T; ++t) phase_dc_refpar_fill<N>(t, stage.data(), start, pf);
+                static_assert(RefparArea<N>::BYTES <= LY::SPEC_BYTES, "the step records fit the spectrum area");
+                unsigned char* area = work.data() + LY::OFF_SPEC;
+                for (int t = 0; t < T; ++t) phase_dc_refpar_seg<N>(t, stage.data(), ta[t & ~3], tb[t & ~3], area);
+                for (int t = 0; t < T; ++t) phase_dc_refpar_walk<N>(t, stage.data(), area);
+                for (int t = 0; t < T; ++t) phase_dc_refpar_fill<N>(t, stage.data(), area, pf);
             } else {
                 for (int t = 0; t < T; ++t) phase_dc_ref_scan<N, DT>(t, stage.data(), pf);
             }
