@@ -775,15 +775,9 @@ OPE_HD void phase_dc_refpar_seg(int t, const unsigned char* stage, int ex_a, int
     }
 }
 
-// The float additions of samples [16j, 16j + 16) of segment q of row `row` onto f
-// (out of line on the device: the walk needs it for a few parts per row only).
+// The float additions of samples [16j, 16j + 16) of segment q of row `row` onto f.
 template <int N>
-#if defined(__CUDACC__)
-__host__ __device__ __noinline__
-#else
-inline
-#endif
-float refpar_add_part(const unsigned char* stage, int row, int q, int j, float f) {
+OPE_HD float refpar_add_part(const unsigned char* stage, int row, int q, int j, float f) {
     float x[16];
     refpar_load8<N>(stage, row, q, 2 * j, x);
     refpar_load8<N>(stage, row, q, 2 * j + 1, x + 8);
@@ -808,7 +802,13 @@ OPE_HD unsigned refpar_walk_parts(const unsigned char* stage, const int4* part, 
 
 // Step 2. Row 0 is walked by thread 0 and row 1 by thread 32 (lane 1 when the
 // team is one warp), so that the rows' part-wise segments do not hold up each
-// other. The segment records are read in blocks of 8 ahead of the block's steps.
+// other. One rolled loop, the next segment's record read ahead of the current
+// step and of the store of its start value (a shared-memory load cannot be
+// moved above a shared-memory store). The walk is a serial chain of a few
+// dependent integer instructions per segment; with the SM's other CTAs issuing
+// beside it, it takes about 7.5 k cycles per pair at N = 2048 (measured; a
+// warp-cooperative form with the records in registers and one shuffle per field
+// and step measured slower, 9.6 k).
 template <int N>
 OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, unsigned char* area) {
     constexpr int WALKER1 = Plan<N>::T >= 64 ? 32 : 1;
@@ -816,22 +816,14 @@ OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, unsigned cha
     const RefparArea<N> A(area);
     const int r = t == 0 ? 0 : 1;
     constexpr int NSEG = RefparArea<N>::NSEG;
-    constexpr int B = NSEG < 8 ? NSEG : 8;
-    static_assert(NSEG % B == 0, "whole blocks of segments");
     unsigned s = 0;
+    int4 g = A.seg[r];
 #pragma unroll 1
-    for (int q0 = 0; q0 < NSEG; q0 += B) {
-        int4 g[B];
-        unsigned st[B];
-#pragma unroll
-        for (int j = 0; j < B; ++j) g[j] = A.seg[2 * (q0 + j) + r];
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            st[j] = s;
-            if (!refpar_step(s, g[j])) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * (q0 + j) + r), r, q0 + j, s);
-        }
-#pragma unroll
-        for (int j = 0; j < B; ++j) A.start[2 * (q0 + j) + r] = st[j];
+    for (int q = 0; q < NSEG; ++q) {
+        const int4 gn = A.seg[2 * (q + 1 < NSEG ? q + 1 : q) + r];
+        A.start[2 * q + r] = s;
+        if (!refpar_step(s, g)) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * q + r), r, q, s);
+        g = gn;
     }
 }
 

@@ -72,6 +72,26 @@ def test_reference_order_exact_prefix_shortcut_bit_identical_to_emulation(cuda, 
     assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
 
 
+@pytest.mark.parametrize("n", [512, 1024, 4096, 8192])
+def test_reference_order_segments_bit_identical_to_emulation(cuda, emu, n):
+    """Full-range 16-bit samples in reference order at every segment count of
+    the kernel's segment form of the float prefix (8 segments per row at
+    N = 512, where one warp walks both rows, to 128 at N = 8192, four records
+    per lane): the GPU's complex bins equal the emulation's (whose k-linearised
+    spectrum equals the reference library's) bit for bit. Rows as in the
+    emulator's structured-row test: constant 65535, constant 32769 (ties),
+    alternating 65535 / 1, values 2 mod 4 near the top, random."""
+    rng = np.random.default_rng(n + 7)
+    i = np.arange(n)
+    raw = np.stack([np.full(n, 65535), np.full(n, 32769), np.where(i % 2 == 1, 65535, 1),
+                    65530 - 4 * rng.integers(0, 8, size=n), rng.integers(0, 65536, size=n),
+                    rng.integers(30000, 65536, size=n)]).astype(np.uint16)
+    spec = spec_for(n, CUBIC, dtype=UINT16, m=raw.shape[0], dc_removal=True, dc_window=64, dc_reference_order=True)
+    g = H.gpu_run(spec, raw, "bins")
+    e = H.emu_run(emu, spec, raw, "bins")
+    assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
+
+
 @pytest.mark.parametrize("interp", INTERPS)
 @pytest.mark.parametrize("n", [512, 2048, 8192])
 def test_image_vs_oracle(cuda, n, interp):
