@@ -800,31 +800,120 @@ OPE_HD unsigned refpar_walk_parts(const unsigned char* stage, const int4* part, 
     return s;
 }
 
-// Step 2. Row 0 is walked by thread 0 and row 1 by thread 32 (lane 1 when the
-// team is one warp), so that the rows' part-wise segments do not hold up each
-// other. One rolled loop, the next segment's record read ahead of the current
-// step and of the store of its start value (a shared-memory load cannot be
-// moved above a shared-memory store). The walk is a serial chain of a few
-// dependent integer instructions per segment; with the SM's other CTAs issuing
-// beside it, it takes about 7.5 k cycles per pair at N = 2048 (measured; a
-// warp-cooperative form with the records in registers and one shuffle per field
-// and step measured slower, 9.6 k).
+#if defined(__CUDA_ARCH__)
+// Consecutive segment records of one binade composed: from a start s with
+// u << 23 <= s < hi, an even s / u adds a, an odd one adds b.
+struct RefparComp {
+    unsigned hi, a, b;
+};
+
+// f first, then g (one u). After f the parity of s / u flips with that of the
+// ulps f added; the composite's bound keeps both parts valid (conservatively,
+// with the larger of f's increments).
+__device__ __forceinline__ RefparComp refpar_compose(RefparComp f, RefparComp g, unsigned u) {
+    RefparComp c;
+    c.a = f.a + ((f.a & u) ? g.b : g.a);
+    c.b = f.b + ((f.b & u) ? g.a : g.b);
+    const unsigned m = f.a > f.b ? f.a : f.b;
+    const unsigned gh = g.hi > m ? g.hi - m : 0u;
+    c.hi = f.hi < gh ? f.hi : gh;
+    return c;
+}
+
+__device__ __forceinline__ RefparComp refpar_shfl_up(RefparComp c, int d) {
+    return RefparComp{__shfl_up_sync(0xffffffffu, c.hi, d), __shfl_up_sync(0xffffffffu, c.a, d),
+                      __shfl_up_sync(0xffffffffu, c.b, d)};
+}
+
+// One warp walks row r, 32 segments at a time, lane L holding segment L's
+// record. Runs of consecutive segments in one binade (one u) are composed by a
+// segmented scan over the lanes; the walk then takes a whole run at once: every
+// lane of the run forms its start value from the run's start and the composite
+// of the run's earlier segments. From the first lane whose composite or own
+// record does not apply (normally a run's last segment, where the walk crosses
+// into the next binade), the segments of that run are walked one at a time,
+// part by part where needed. Every lane keeps the same walk value, so the warp
+// never diverges.
+template <int N>
+__device__ __forceinline__ void refpar_walk_scan(int lane, int r, const unsigned char* stage,
+                                                 const RefparArea<N>& A) {
+    constexpr int NSEG = RefparArea<N>::NSEG;
+    constexpr int M = (NSEG + 31) / 32;
+    constexpr int J = NSEG < 32 ? NSEG : 32;  // segments per block of lanes
+    constexpr unsigned LIVE = J == 32 ? 0xffffffffu : ((1u << J) - 1u);
+    unsigned s = 0;
+#pragma unroll 1
+    for (int m = 0; m < M; ++m) {
+        const int q = 32 * m + lane;
+        const int4 g = lane < J ? A.seg[2 * q + r] : make_int4(0, 0, 0, 0);
+        const unsigned u = (unsigned)g.y;
+        const unsigned uprev = __shfl_up_sync(0xffffffffu, u, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || u != uprev) & LIVE;
+        const int rs = 31 - __clz((int)(heads & (0xffffffffu >> (31 - lane))));  // this lane's run start
+        RefparComp c{(unsigned)g.x, (unsigned)g.z, (unsigned)g.w};
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const RefparComp o = refpar_shfl_up(c, d);
+            if (lane - d >= rs) c = refpar_compose(o, c, u);
+        }
+        const RefparComp ex = refpar_shfl_up(c, 1);  // the run's segments before this lane
+        int L = 0;
+        while (L < J) {
+            if ((heads >> L) & 1u) {
+                const unsigned later = heads & ~((2u << L) - 1u);
+                const int end = later ? __ffs((int)later) - 1 : J;
+                const bool in = lane >= L && lane < end;
+                unsigned my = s;
+                bool ok = s >= (u << 23);
+                if (lane > L) {
+                    ok = ok && s < ex.hi;
+                    my = s + ((s & u) ? ex.b : ex.a);
+                }
+                ok = ok && my < (unsigned)g.x;
+                const unsigned bad = __ballot_sync(0xffffffffu, in && !ok);
+                const int stop = bad ? __ffs((int)bad) - 1 : end;
+                if (lane >= L && lane < stop) A.start[2 * q + r] = my;
+                if (stop > L) s = __shfl_sync(0xffffffffu, my + ((my & u) ? (unsigned)g.w : (unsigned)g.z), stop - 1);
+                L = stop;
+                if (stop == end) continue;
+            }
+            // segment L on its own: its record, else part by part
+            const int4 gl = make_int4(__shfl_sync(0xffffffffu, g.x, L), __shfl_sync(0xffffffffu, g.y, L),
+                                      __shfl_sync(0xffffffffu, g.z, L), __shfl_sync(0xffffffffu, g.w, L));
+            const int ql = 32 * m + L;
+            if (lane == 0) A.start[2 * ql + r] = s;
+            if (!refpar_step(s, gl)) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * ql + r), r, ql, s);
+            ++L;
+        }
+    }
+}
+#endif
+
+// Step 2. Each row's segments in order from 0: one record step per segment; a
+// segment whose record does not apply is walked part by part
+// (refpar_walk_parts). On the device warp r walks row r by runs
+// (refpar_walk_scan; one warp walks both rows in turn when the team is one warp);
+// the host walk, one thread per row, gives the same values.
 template <int N>
 OPE_HD void phase_dc_refpar_walk(int t, const unsigned char* stage, unsigned char* area) {
-    constexpr int WALKER1 = Plan<N>::T >= 64 ? 32 : 1;
-    if (t != 0 && t != WALKER1) return;
     const RefparArea<N> A(area);
-    const int r = t == 0 ? 0 : 1;
-    constexpr int NSEG = RefparArea<N>::NSEG;
-    unsigned s = 0;
-    int4 g = A.seg[r];
-#pragma unroll 1
-    for (int q = 0; q < NSEG; ++q) {
-        const int4 gn = A.seg[2 * (q + 1 < NSEG ? q + 1 : q) + r];
-        A.start[2 * q + r] = s;
-        if (!refpar_step(s, g)) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * q + r), r, q, s);
-        g = gn;
+#if defined(__CUDA_ARCH__)
+    const int warp = t >> 5, lane = t & 31;
+    if (Plan<N>::T >= 64) {
+        if (warp < 2) refpar_walk_scan<N>(lane, warp, stage, A);
+    } else {
+        refpar_walk_scan<N>(lane, 0, stage, A);
+        refpar_walk_scan<N>(lane, 1, stage, A);
     }
+#else
+    if (t > 1) return;
+    const int r = t;
+    unsigned s = 0;
+    for (int q = 0; q < RefparArea<N>::NSEG; ++q) {
+        A.start[2 * q + r] = s;
+        if (!refpar_step(s, A.seg[2 * q + r])) s = refpar_walk_parts<N>(stage, A.part + 8 * (2 * q + r), r, q, s);
+    }
+#endif
 }
 
 // Step 3. Segment q's four threads write its prefix entries: thread 4q + 2r + h
