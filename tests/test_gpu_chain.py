@@ -92,6 +92,21 @@ def test_reference_order_segments_bit_identical_to_emulation(cuda, emu, n):
     assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
 
 
+@pytest.mark.parametrize("dtype", [UINT8, UINT16, FLOAT32])
+@pytest.mark.parametrize("n", [512, 1024, 4096, 8192])
+def test_exact_sum_dc_removal_bit_identical_to_emulation(cuda, emu, n, dtype):
+    """Rolling-average DC removal with exact window sums at every length: the
+    interior chunks' window means come from paired prefix entries (and, for 8-
+    and 16-bit samples, sums converted as (2^23 + S) - 2^23), the edge chunks'
+    from single entries with the correctly rounded division; the GPU's complex
+    bins equal the emulation's bit for bit."""
+    spec = spec_for(n, CUBIC, dtype=dtype, m=5, dc_removal=True, dc_window=64)
+    raw = H.random_raw(spec, seed=n + 11 * dtype)
+    g = H.gpu_run(spec, raw, "bins")
+    e = H.emu_run(emu, spec, raw, "bins")
+    assert np.array_equal(g.astype(np.complex64), e.astype(np.complex64))
+
+
 @pytest.mark.parametrize("interp", INTERPS)
 @pytest.mark.parametrize("n", [512, 2048, 8192])
 def test_image_vs_oracle(cuda, n, interp):
